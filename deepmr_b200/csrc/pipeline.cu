@@ -1,0 +1,508 @@
+// NUFFT pipelines around cuFFT: apodisation + zero-pad + ifftshift fused into
+// one kernel before the forward transform, fftshift + crop + 1/G +
+// apodisation fused into one kernel after the inverse transform, and the
+// Toeplitz self-adjoint (pad, FFT, kernel multiply, inverse FFT, crop).
+//
+// Reference: _apply_nufft / _apply_nufft_adj / _apply_nufft_selfadj
+// (src/deepmr/fft/nufft.py:423-669), resize (src/deepmr/_signal/resize.py:11-102),
+// centred fft/ifft (src/deepmr/fft/fft.py:9-167), plan_toeplitz
+// (src/deepmr/fft/toeplitz.py:131-155).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+#include "plan.cuh"
+
+namespace dmr {
+
+int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
+                    const float *weight, int wpb, cudaStream_t st);
+int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                  const float *weight, int wpb, int det, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Generic centred resize with index rolls and per-axis apodisation:
+//   output physical q -> logical lo = (q + oroll) mod O
+//   input logical li = lo - so + si, valid for so <= lo < so + cp (resize.py:86-97)
+//   input physical = (li + iroll) mod I
+//   out = in * scale * apod_x * apod_y * apod_z (apodisation of the image side,
+//   applied axis by axis from the last like _apodize, nufft.py:425-445)
+// ---------------------------------------------------------------------------
+struct ResizeArgs {
+    int O[3], I[3];
+    int oroll[3], iroll[3];
+    int so[3], si[3], cp[3];
+    const float *apod[3];
+    int apod_on_output;
+    float scale;
+    int64_t nbatch;
+    int64_t osize, isize;
+    int in_real;
+};
+
+__global__ void resize_kernel(ResizeArgs r, const void *__restrict__ in, float2 *__restrict__ out)
+{
+    for (int64_t bi = blockIdx.y; bi < r.nbatch; bi += gridDim.y) {
+        const int64_t ibase = bi * r.isize;
+        const int64_t obase = bi * r.osize;
+        for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < r.osize;
+             q += (int64_t)gridDim.x * blockDim.x) {
+            const int qx = (int)(q % r.O[0]);
+            const int64_t t = q / r.O[0];
+            const int qy = (int)(t % r.O[1]);
+            const int qz = (int)(t / r.O[1]);
+            const int qq[3] = {qx, qy, qz};
+            bool valid = true;
+            int li[3], lo[3], pi[3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                lo[a] = qq[a] + r.oroll[a];
+                if (lo[a] >= r.O[a]) lo[a] -= r.O[a];
+                valid = valid && lo[a] >= r.so[a] && lo[a] < r.so[a] + r.cp[a];
+                li[a] = lo[a] - r.so[a] + r.si[a];
+                pi[a] = li[a] + r.iroll[a];
+                if (pi[a] >= r.I[a]) pi[a] -= r.I[a];
+            }
+            float2 v = make_float2(0.0f, 0.0f);
+            if (valid) {
+                const int64_t ii = ibase + ((int64_t)pi[2] * r.I[1] + pi[1]) * r.I[0] + pi[0];
+                if (r.in_real) v.x = reinterpret_cast<const float *>(in)[ii];
+                else v = reinterpret_cast<const float2 *>(in)[ii];
+                if (r.scale != 1.0f) {
+                    v.x *= r.scale;
+                    v.y *= r.scale;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    if (r.apod[a]) {
+                        const float ap = r.apod[a][r.apod_on_output ? lo[a] : li[a]];
+                        v.x *= ap;
+                        v.y *= ap;
+                    }
+                }
+            }
+            out[obase + q] = v;
+        }
+    }
+}
+
+// resize offsets of resize.py:86-91 for one axis of extent i -> o
+static void resize_offsets(int i, int o, int &si, int &so, int &cp)
+{
+    si = std::max(i / 2 - o / 2, 0);
+    so = std::max(o / 2 - i / 2, 0);
+    cp = std::min(i - si, o - so);
+}
+
+static int launch_resize(const ResizeArgs &r, const void *in, float2 *out, cudaStream_t st)
+{
+    if (r.nbatch == 0 || r.osize == 0) return DMR_OK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int threads = 256;
+    const int64_t want = ceil_div(r.osize, threads);
+    const int64_t gy = std::min<int64_t>(r.nbatch, 65535);
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8 / std::max<int64_t>(1, std::min<int64_t>(gy, 8)) + 1));
+    dim3 grd((unsigned)std::min<int64_t>(gx, want), (unsigned)gy);
+    resize_kernel<<<grd, threads, 0, st>>>(r, in, out);
+    DMR_LAUNCHED("resize_kernel");
+    return DMR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// cuFFT plan cache (process-wide), work area supplied by the caller
+// ---------------------------------------------------------------------------
+static std::mutex g_fft_mu;
+static std::map<std::tuple<int, int, int, int, int, int64_t>, std::shared_ptr<FftPlan>> g_fft;
+
+std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t batch, int *err)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int d[3] = {1, 1, 1};
+    for (int i = 0; i < ndim; i++) d[i] = dims_zyx[i];
+    auto key = std::make_tuple(dev, ndim, d[0], d[1], d[2], batch);
+    std::lock_guard<std::mutex> lk(g_fft_mu);
+    auto it = g_fft.find(key);
+    if (it != g_fft.end()) return it->second;
+    auto fp = std::make_shared<FftPlan>();
+    long long n[3];
+    long long dist = 1;
+    for (int i = 0; i < ndim; i++) {
+        n[i] = dims_zyx[i];
+        dist *= n[i];
+    }
+    cufftResult r = cufftCreate(&fp->handle);
+    if (r == CUFFT_SUCCESS) r = cufftSetAutoAllocation(fp->handle, 0);
+    size_t ws = 0;
+    if (r == CUFFT_SUCCESS)
+        r = cufftMakePlanMany64(fp->handle, ndim, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_C2C,
+                                batch, &ws);
+    if (r != CUFFT_SUCCESS) {
+        set_error("cuFFT plan creation failed (code %d) for batch %lld", (int)r, (long long)batch);
+        *err = DMR_ERR_CUFFT;
+        if (fp->handle) cufftDestroy(fp->handle);
+        return nullptr;
+    }
+    fp->work_bytes = ws;
+    g_fft[key] = fp;
+    *err = DMR_OK;
+    return fp;
+}
+
+static int fft_exec(FftPlan &fp, float2 *data, int direction, void *work, cudaStream_t st)
+{
+    std::lock_guard<std::mutex> lk(fp.mu);
+    cufftResult r = cufftSetStream(fp.handle, st);
+    if (r == CUFFT_SUCCESS) r = cufftSetWorkArea(fp.handle, work);
+    if (r == CUFFT_SUCCESS)
+        r = cufftExecC2C(fp.handle, (cufftComplex *)data, (cufftComplex *)data, direction);
+    DMR_CHECK(r == CUFFT_SUCCESS, DMR_ERR_CUFFT, "cufftExecC2C failed (code %d)", (int)r);
+    return DMR_OK;
+}
+
+static void zyx_dims(const Geom &g, const int *ext, int out[3])
+{
+    for (int i = 0; i < g.ndim; i++) out[i] = ext[g.ndim - 1 - i];
+}
+
+struct NufftWs {
+    float2 *grid;
+    void *fft_work;
+    std::shared_ptr<FftPlan> fft;
+};
+
+static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, NufftWs &out, size_t *need)
+{
+    const Geom &g = p->g;
+    int dims[3];
+    zyx_dims(g, g.G, dims);
+    int err = DMR_OK;
+    auto fp = get_fft_plan(g.ndim, dims, batch * g.nframes, &err);
+    if (!fp) return err;
+    const size_t grid_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
+    const size_t total = grid_bytes + align_up(fp->work_bytes, 256);
+    if (need) *need = total;
+    if (!ws) return DMR_OK;
+    DMR_CHECK(ws_bytes >= total, DMR_ERR_WORKSPACE, "workspace too small: %zu < %zu", ws_bytes, total);
+    DMR_CHECK(((uintptr_t)ws & 255) == 0, DMR_ERR_INVALID, "workspace must be 256-byte aligned");
+    out.grid = (float2 *)ws;
+    out.fft_work = fp->work_bytes ? (char *)ws + grid_bytes : nullptr;
+    out.fft = fp;
+    return DMR_OK;
+}
+
+__global__ void cmul_kernel(float2 *__restrict__ data, const float2 *__restrict__ kern, int64_t ksize,
+                            int64_t nk, int64_t nbatch, float s)
+{
+    const int64_t n = ksize * nbatch;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t bi = e / ksize;
+        const int64_t q = e - bi * ksize;
+        const float2 k = kern[(bi % nk) * ksize + q];
+        const float2 d = data[e];
+        // kernel value times spectrum (toeplitz.py:86), then the two orthonormal 1/sqrt(K)
+        float2 o = make_float2(k.x * d.x - k.y * d.y, k.x * d.y + k.y * d.x);
+        o.x *= s;
+        o.y *= s;
+        data[e] = o;
+    }
+}
+
+// mean of |k| over the non-zero entries (toeplitz.py:152), two-stage in float64
+__global__ void absmean_partial_kernel(const float2 *__restrict__ k, int64_t n, double *__restrict__ sums,
+                                       unsigned long long *__restrict__ counts)
+{
+    double s = 0.0;
+    unsigned long long c = 0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = k[e];
+        if (v.x != 0.0f || v.y != 0.0f) {
+            s += (double)hypotf(v.x, v.y);
+            c++;
+        }
+    }
+    __shared__ double ss[256];
+    __shared__ unsigned long long sc[256];
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            ss[threadIdx.x] += ss[threadIdx.x + h];
+            sc[threadIdx.x] += sc[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        sums[blockIdx.x] = ss[0];
+        counts[blockIdx.x] = sc[0];
+    }
+}
+
+__global__ void normalise_kernel(float2 *__restrict__ k, int64_t n, const double *__restrict__ sums,
+                                 const unsigned long long *__restrict__ counts, int nparts)
+{
+    __shared__ float inv_mean;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        unsigned long long c = 0;
+        for (int i = 0; i < nparts; i++) {
+            s += sums[i];
+            c += counts[i];
+        }
+        // mean of an empty selection is NaN in the reference; keep that
+        const float mean = c ? (float)(s / (double)c) : __int_as_float(0x7fc00000);
+        inv_mean = mean;
+    }
+    __syncthreads();
+    const float m = inv_mean;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        float2 v = k[e];
+        v.x = v.x / m;
+        v.y = v.y / m;
+        // torch.nan_to_num: NaN -> 0, +-inf -> +-FLT_MAX
+        if (isnan(v.x)) v.x = 0.0f; else if (isinf(v.x)) v.x = v.x > 0 ? 3.402823466e38f : -3.402823466e38f;
+        if (isnan(v.y)) v.y = 0.0f; else if (isinf(v.y)) v.y = v.y > 0 ? 3.402823466e38f : -3.402823466e38f;
+        k[e] = v;
+    }
+}
+
+constexpr int kReduceBlocks = 296;
+
+static int elem_blocks(int64_t n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 8));
+}
+
+}  // namespace dmr
+
+using namespace dmr;
+
+extern "C" int dmr_nufft_workspace_bytes(dmr_plan *p, int64_t batch, size_t *bytes)
+{
+    DMR_CHECK(p && bytes && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    NufftWs w;
+    return nufft_ws(p, batch, nullptr, 0, w, bytes);
+}
+
+extern "C" int dmr_nufft_forward(dmr_plan *p, const void *image, int image_real, void *kspace,
+                                 int64_t batch, const float *weight, int weight_per_batch,
+                                 void *workspace, size_t workspace_bytes, void *stream)
+{
+    DMR_CHECK(p && image && kspace && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geom &g = p->g;
+    NufftWs w;
+    DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    for (int a = 0; a < 3; a++) {
+        r.O[a] = g.G[a];
+        r.I[a] = g.N[a];
+        r.oroll[a] = g.half[a];  // X[q] = P[(q + G//2) mod G]: ifftshift folded in
+        r.iroll[a] = 0;
+        resize_offsets(g.N[a], g.G[a], r.si[a], r.so[a], r.cp[a]);
+        r.apod[a] = (a < g.ndim && g.W[a] != 1) ? p->apod[a] : nullptr;
+    }
+    r.apod_on_output = 0;
+    r.scale = 1.0f;
+    r.nbatch = batch * g.nframes;
+    r.osize = g.gsize;
+    r.isize = g.isize;
+    r.in_real = image_real;
+    DMR_TRY(launch_resize(r, image, w.grid, st));
+    DMR_TRY(fft_exec(*w.fft, w.grid, CUFFT_FORWARD, w.fft_work, st));
+    return interp_dispatch(p, w.grid, (float2 *)kspace, batch, weight, weight_per_batch, st);
+}
+
+extern "C" int dmr_nufft_adjoint(dmr_plan *p, const void *kspace, int kspace_real, void *image,
+                                 int64_t batch, const float *weight, int weight_per_batch,
+                                 int deterministic, void *workspace, size_t workspace_bytes,
+                                 void *stream)
+{
+    DMR_CHECK(p && image && kspace && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geom &g = p->g;
+    NufftWs w;
+    DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
+    DMR_TRY(grid_dispatch(p, kspace, kspace_real, w.grid, batch, weight, weight_per_batch,
+                          deterministic, st));
+    DMR_TRY(fft_exec(*w.fft, w.grid, CUFFT_INVERSE, w.fft_work, st));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    for (int a = 0; a < 3; a++) {
+        r.O[a] = g.N[a];
+        r.I[a] = g.G[a];
+        r.oroll[a] = 0;
+        r.iroll[a] = g.G[a] - g.half[a];  // fftshift folded in: centred li at (li - G//2) mod G
+        if (r.iroll[a] == g.G[a]) r.iroll[a] = 0;
+        resize_offsets(g.G[a], g.N[a], r.si[a], r.so[a], r.cp[a]);
+        r.apod[a] = (a < g.ndim && g.W[a] != 1) ? p->apod[a] : nullptr;
+    }
+    r.apod_on_output = 1;
+    r.scale = (float)(1.0 / (double)g.gsize);  // ifftn norm="backward" (nufft.py:587)
+    r.nbatch = batch * g.nframes;
+    r.osize = g.isize;
+    r.isize = g.gsize;
+    r.in_real = 0;
+    return launch_resize(r, w.grid, (float2 *)image, st);
+}
+
+static int toep_dims(int ndim, const int32_t *kshape, int dims[3], int64_t &ksize)
+{
+    DMR_CHECK(ndim >= 1 && ndim <= 3 && kshape, DMR_ERR_INVALID, "bad Toeplitz shape");
+    ksize = 1;
+    for (int i = 0; i < ndim; i++) {
+        DMR_CHECK(kshape[i] >= 1, DMR_ERR_INVALID, "bad Toeplitz shape");
+        dims[i] = kshape[i];
+        ksize *= kshape[i];
+    }
+    return DMR_OK;
+}
+
+extern "C" int dmr_toeplitz_workspace_bytes(int ndim, const int32_t *kshape, int64_t batch, size_t *bytes)
+{
+    DMR_CHECK(bytes && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    int dims[3];
+    int64_t ksize;
+    DMR_TRY(toep_dims(ndim, kshape, dims, ksize));
+    int err = DMR_OK;
+    auto fp = get_fft_plan(ndim, dims, batch, &err);
+    if (!fp) return err;
+    *bytes = align_up((size_t)batch * ksize * sizeof(float2), 256) + align_up(fp->work_bytes, 256) +
+             align_up(kReduceBlocks * (sizeof(double) + sizeof(unsigned long long)), 256);
+    return DMR_OK;
+}
+
+// carve the Toeplitz workspace: data | cuFFT work | reduction scratch
+static int toep_ws(int ndim, const int32_t *kshape, int64_t batch, void *ws, size_t ws_bytes,
+                   float2 **data, void **work, double **sums, unsigned long long **counts,
+                   std::shared_ptr<FftPlan> &fp)
+{
+    int dims[3];
+    int64_t ksize;
+    DMR_TRY(toep_dims(ndim, kshape, dims, ksize));
+    int err = DMR_OK;
+    fp = get_fft_plan(ndim, dims, batch, &err);
+    if (!fp) return err;
+    const size_t a = align_up((size_t)batch * ksize * sizeof(float2), 256);
+    const size_t b = align_up(fp->work_bytes, 256);
+    const size_t c = align_up(kReduceBlocks * (sizeof(double) + sizeof(unsigned long long)), 256);
+    DMR_CHECK(ws && ws_bytes >= a + b + c, DMR_ERR_WORKSPACE, "workspace too small: %zu < %zu",
+              ws_bytes, a + b + c);
+    DMR_CHECK(((uintptr_t)ws & 255) == 0, DMR_ERR_INVALID, "workspace must be 256-byte aligned");
+    *data = (float2 *)ws;
+    *work = fp->work_bytes ? (char *)ws + a : nullptr;
+    *sums = (double *)((char *)ws + a + b);
+    *counts = (unsigned long long *)(*sums + kReduceBlocks);
+    return DMR_OK;
+}
+
+extern "C" int dmr_toeplitz_finalize(int ndim, const int32_t *kshape, int64_t nk, const void *psf,
+                                     void *kernel, void *workspace, size_t workspace_bytes,
+                                     void *stream)
+{
+    DMR_CHECK(psf && kernel && nk >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    float2 *data;
+    void *work;
+    double *sums;
+    unsigned long long *counts;
+    std::shared_ptr<FftPlan> fp;
+    DMR_TRY(toep_ws(ndim, kshape, nk, workspace, workspace_bytes, &data, &work, &sums, &counts, fp));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    int64_t ksize = 1;
+    for (int a = 0; a < 3; a++) {
+        const int ext = a < ndim ? kshape[ndim - 1 - a] : 1;
+        r.O[a] = r.I[a] = r.cp[a] = ext;
+        r.iroll[a] = ext / 2;  // ifftshift: out[q] = in[(q + n//2) mod n]
+        if (r.iroll[a] == ext) r.iroll[a] = 0;
+        ksize *= ext;
+    }
+    r.scale = 1.0f;
+    r.nbatch = nk;
+    r.osize = r.isize = ksize;
+    DMR_TRY(launch_resize(r, psf, data, st));
+    DMR_TRY(fft_exec(*fp, data, CUFFT_FORWARD, work, st));
+    // fftshift then ifftshift cancel; the orthonormal 1/sqrt(K) cancels in the
+    // normalisation but is applied so zero tests see the same values
+    const float ortho = (float)(1.0 / std::sqrt((double)ksize));
+    const int64_t n = nk * ksize;
+    ResizeArgs s;
+    memset(&s, 0, sizeof(s));
+    for (int a = 0; a < 3; a++) {
+        s.O[a] = s.I[a] = s.cp[a] = r.O[a];
+    }
+    s.scale = ortho;
+    s.nbatch = nk;
+    s.osize = s.isize = ksize;
+    DMR_TRY(launch_resize(s, data, (float2 *)kernel, st));
+    absmean_partial_kernel<<<kReduceBlocks, 256, 0, st>>>((const float2 *)kernel, n, sums, counts);
+    DMR_LAUNCHED("absmean_partial_kernel");
+    normalise_kernel<<<elem_blocks(n), 256, 0, st>>>((float2 *)kernel, n, sums, counts, kReduceBlocks);
+    DMR_LAUNCHED("normalise_kernel");
+    return DMR_OK;
+}
+
+extern "C" int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t *ishape,
+                                  const void *kernel, int64_t nk, const void *image, int image_real,
+                                  void *out, int64_t batch, void *workspace, size_t workspace_bytes,
+                                  void *stream)
+{
+    DMR_CHECK(kernel && image && out && ishape && nk >= 1 && batch >= 1, DMR_ERR_INVALID,
+              "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    float2 *data;
+    void *work;
+    double *sums;
+    unsigned long long *counts;
+    std::shared_ptr<FftPlan> fp;
+    DMR_TRY(toep_ws(ndim, kshape, batch, workspace, workspace_bytes, &data, &work, &sums, &counts, fp));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    int64_t ksize = 1, isize = 1;
+    for (int a = 0; a < 3; a++) {
+        const int K = a < ndim ? kshape[ndim - 1 - a] : 1;
+        const int N = a < ndim ? ishape[ndim - 1 - a] : 1;
+        r.O[a] = K;
+        r.I[a] = N;
+        resize_offsets(N, K, r.si[a], r.so[a], r.cp[a]);
+        ksize *= K;
+        isize *= N;
+    }
+    r.scale = 1.0f;
+    r.nbatch = batch;
+    r.osize = ksize;
+    r.isize = isize;
+    r.in_real = image_real;
+    DMR_TRY(launch_resize(r, image, data, st));
+    DMR_TRY(fft_exec(*fp, data, CUFFT_FORWARD, work, st));
+    const int64_t n = batch * ksize;
+    cmul_kernel<<<elem_blocks(n), 256, 0, st>>>(data, (const float2 *)kernel, ksize, nk, batch,
+                                                (float)(1.0 / (double)ksize));
+    DMR_LAUNCHED("cmul_kernel");
+    DMR_TRY(fft_exec(*fp, data, CUFFT_INVERSE, work, st));
+    ResizeArgs c;
+    memset(&c, 0, sizeof(c));
+    for (int a = 0; a < 3; a++) {
+        c.O[a] = r.I[a];
+        c.I[a] = r.O[a];
+        resize_offsets(c.I[a], c.O[a], c.si[a], c.so[a], c.cp[a]);
+    }
+    c.scale = 1.0f;
+    c.nbatch = batch;
+    c.osize = isize;
+    c.isize = ksize;
+    return launch_resize(c, data, (float2 *)out, st);
+}

@@ -1,0 +1,80 @@
+// Device-resident NUFFT plan: geometry, bin structure and the sorted samples.
+#pragma once
+
+#include <cufft.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dmr {
+
+// Geometry passed by value to every kernel. Axis index 0 = x (fastest),
+// 1 = y, 2 = z; unused axes have G = N = W = T = nb = 1.
+struct Geom {
+    int ndim;
+    int G[3];       // oversampled grid extent
+    int N[3];       // image extent
+    int W[3];       // kernel width (1: Cartesian axis, nearest node by truncation)
+    int half[3];    // G // 2 (fftshift offset)
+    int T[3];       // bin / tile extent
+    int nb[3];      // bins per axis
+    float beta[3];  // Kaiser-Bessel beta
+    double inv_hw[3];  // 1 / (W / 2)
+    int nbins;      // bins per frame
+    int nframes;
+    int64_t gsize;  // grid points per (batch, frame)
+    int64_t isize;  // image points per (batch, frame)
+    int64_t total;  // samples over all frames
+};
+
+// One block-level unit of interpolation / atomic-gridding work: a chunk of
+// the samples of one bin (bin id includes the frame: f * nbins + local).
+struct WorkItem {
+    int bin;
+    int begin;
+    int end;
+};
+
+struct FftPlan {
+    cufftHandle handle = 0;
+    size_t work_bytes = 0;
+    std::mutex mu;
+};
+
+// Process-wide cache of cuFFT plans keyed by (device, rank, dims, batch).
+std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t batch, int *err);
+
+}  // namespace dmr
+
+struct dmr_plan {
+    dmr::Geom g;
+    int device;
+    double scale;                       // kernel-sum normalisation
+    std::vector<int64_t> frame_offsets;  // host CSR
+    float os[3];
+    // device buffers
+    float *scoord[3] = {nullptr, nullptr, nullptr};  // sorted rescaled coordinates
+    int32_t *sidx = nullptr;            // sorted position -> global sample index
+    int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
+    dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
+    int nwork = 0;
+    int32_t *tiles = nullptr;           // owner-gridding tile order (heavy first)
+    int ntiles = 0;
+    float *apod[3] = {nullptr, nullptr, nullptr};  // per-axis apodisation (image index)
+
+    ~dmr_plan()
+    {
+        for (int a = 0; a < 3; a++) {
+            cudaFree(scoord[a]);
+            cudaFree(apod[a]);
+        }
+        cudaFree(sidx);
+        cudaFree(bin_start);
+        cudaFree(work);
+        cudaFree(tiles);
+    }
+};

@@ -1,0 +1,688 @@
+// Interpolation (oversampled grid -> samples) and gridding (samples -> grid)
+// with Kaiser-Bessel weights evaluated on the fly.
+//
+// Reference: apply_interpolation / apply_gridding and their Numba kernels
+// (src/deepmr/fft/_interp/interp.py:14-227, 415-749;
+//  src/deepmr/fft/_interp/grid.py:14-284, 424-1168). The reference launches
+// one thread per (frame, batch, sample) over precomputed (F, M, W) tables and
+// grids with two global float atomics per complex tap. Here samples are
+// sorted by spatial bin (the plan), one thread block stages the bin's grid
+// tile (plus the kernel halo) in shared memory for a chunk of coils, and a
+// warp processes 32/CC samples x CC coils at a time, so each sample's weights
+// are computed once per coil chunk and the grid is read coalesced.
+//
+// Grid layout everywhere: (batch, nframes, *G) complex64 in FFT order — the
+// centred index c of an axis is stored at (c - G//2) mod G — so the fftshift
+// of the reference's centred FFT (src/deepmr/fft/fft.py:77-80) costs nothing.
+#include <algorithm>
+
+#include "kb.cuh"
+#include "plan.cuh"
+
+namespace dmr {
+
+__device__ __forceinline__ int first_tap_dev(float k, int W)
+{
+    if (W == 1) return (int)k;  // Cartesian axis: truncation (plan.py:117-121)
+    return (int)ceil((double)k - 0.5 * (double)W);
+}
+
+// Kernel weight of tap i for a sample at rescaled coordinate k with first tap x0
+// (plan.py:260-268): KB(((x0 + i) - k) / (W/2)); 1 on Cartesian axes.
+__device__ __forceinline__ float tap_weight(int x0, int i, float k, int W, double inv_hw, float beta)
+{
+    if (W == 1) return 1.0f;
+    const double u = ((double)(x0 + i) - (double)k) * inv_hw;
+    return kb_f32((float)u, beta);
+}
+
+template <int NDIM, int WMAX>
+struct Meta {
+    // samples staged per batch (sized so the weight table stays ~12 KB)
+    static constexpr int SB = (NDIM * WMAX <= 16) ? 256 : (NDIM * WMAX <= 32 ? 128 : 64);
+    static constexpr int NW = NDIM * WMAX;
+    static size_t bytes() { return (size_t)SB * (NW * sizeof(float) + 2 * sizeof(int)); }
+};
+
+__device__ __forceinline__ void tile_origin(const Geom &g, int lb, int org[3])
+{
+    org[0] = (lb % g.nb[0]) * g.T[0];
+    org[1] = ((lb / g.nb[0]) % g.nb[1]) * g.T[1];
+    org[2] = (lb / (g.nb[0] * g.nb[1])) * g.T[2];
+}
+
+// Stage per-sample data of samples [base, base+n) of a bin whose tile starts
+// at org: weights (NDIM x WMAX), linear offset of the first tap inside the
+// (T + W - 1)^NDIM region, and the global sample index.
+template <int NDIM, int WMAX>
+__device__ __forceinline__ void stage_samples(const Geom &g, const int org[3], int base, int n,
+                                              const float *__restrict__ sc0,
+                                              const float *__restrict__ sc1,
+                                              const float *__restrict__ sc2,
+                                              const int32_t *__restrict__ sidx, int R0, int R1,
+                                              float *wts, int *off, int *gi)
+{
+    constexpr int NW = NDIM * WMAX;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int j = base + t;
+        const float k[3] = {sc0[j], NDIM > 1 ? sc1[j] : 0.0f, NDIM > 2 ? sc2[j] : 0.0f};
+        int l[3] = {0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NDIM; a++) {
+            const int x0 = first_tap_dev(k[a], g.W[a]);
+            l[a] = pmod(x0, g.G[a]) - org[a];
+#pragma unroll
+            for (int i = 0; i < WMAX; i++)
+                if (i < g.W[a]) wts[t * NW + a * WMAX + i] = tap_weight(x0, i, k[a], g.W[a], g.inv_hw[a], g.beta[a]);
+        }
+        off[t] = (l[2] * R1 + l[1]) * R0 + l[0];
+        gi[t] = sidx[j];
+    }
+}
+
+// Sum over the taps of one sample: sum_z w_z sum_y w_y sum_x w_x tile[z][y][x].
+// Weights come from the staged table `w` (NDIM x WMAX); the x loop is fully
+// unrolled with x weights in registers, outer loops are unrolled for WMAX <= 4.
+template <int NDIM, int WMAX>
+__device__ __forceinline__ float2 gather_taps(const float2 *tp, const float *w, int Wx, int Wy, int Wz,
+                                              int R0, int R1)
+{
+    constexpr int UO = WMAX <= 4 ? WMAX : 1;
+    float wx[WMAX];
+#pragma unroll
+    for (int i = 0; i < WMAX; i++) wx[i] = i < Wx ? w[i] : 0.0f;
+    float ar = 0.0f, ai = 0.0f;
+    auto row_sum = [&](const float2 *row, float &rr, float &ri) {
+#pragma unroll
+        for (int ix = 0; ix < WMAX; ix++)
+            if (ix < Wx) {
+                const float2 v = row[ix];
+                rr += wx[ix] * v.x;
+                ri += wx[ix] * v.y;
+            }
+    };
+    if (NDIM == 1) {
+        row_sum(tp, ar, ai);
+    } else if (NDIM == 2) {
+#pragma unroll UO
+        for (int iy = 0; iy < WMAX; iy++) {
+            if (iy >= Wy) break;
+            float rr = 0.0f, ri = 0.0f;
+            row_sum(tp + iy * R0, rr, ri);
+            const float wy = w[WMAX + iy];
+            ar += wy * rr;
+            ai += wy * ri;
+        }
+    } else {
+#pragma unroll UO
+        for (int iz = 0; iz < WMAX; iz++) {
+            if (iz >= Wz) break;
+            const float wz = w[2 * WMAX + iz];
+#pragma unroll UO
+            for (int iy = 0; iy < WMAX; iy++) {
+                if (iy >= Wy) break;
+                float rr = 0.0f, ri = 0.0f;
+                row_sum(tp + (iz * R1 + iy) * R0, rr, ri);
+                const float wzy = wz * w[WMAX + iy];
+                ar += wzy * rr;
+                ai += wzy * ri;
+            }
+        }
+    }
+    return make_float2(ar, ai);
+}
+
+// Spread one sample value v over its taps with shared-memory atomics; the tap
+// weight is formed like the reference ((w_z * w_y) * w_x, grid.py:262-280).
+template <int NDIM, int WMAX>
+__device__ __forceinline__ void scatter_taps(float2 *tp, const float *w, float2 v, int Wx, int Wy, int Wz,
+                                             int R0, int R1)
+{
+    constexpr int UO = WMAX <= 4 ? WMAX : 1;
+    float wx[WMAX];
+#pragma unroll
+    for (int i = 0; i < WMAX; i++) wx[i] = i < Wx ? w[i] : 0.0f;
+    auto row_add = [&](float2 *row, float wo) {
+#pragma unroll
+        for (int ix = 0; ix < WMAX; ix++)
+            if (ix < Wx) {
+                const float wv = NDIM == 1 ? wx[ix] : wo * wx[ix];
+                atomicAdd(&row[ix].x, wv * v.x);
+                atomicAdd(&row[ix].y, wv * v.y);
+            }
+    };
+    if (NDIM == 1) {
+        row_add(tp, 1.0f);
+    } else if (NDIM == 2) {
+#pragma unroll UO
+        for (int iy = 0; iy < WMAX; iy++) {
+            if (iy >= Wy) break;
+            row_add(tp + iy * R0, w[WMAX + iy]);
+        }
+    } else {
+#pragma unroll UO
+        for (int iz = 0; iz < WMAX; iz++) {
+            if (iz >= Wz) break;
+            const float wz = w[2 * WMAX + iz];
+#pragma unroll UO
+            for (int iy = 0; iy < WMAX; iy++) {
+                if (iy >= Wy) break;
+                row_add(tp + (iz * R1 + iy) * R0, wz * w[WMAX + iy]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Interpolation: grid -> samples, y = (sum_taps w * grid) / scale * weight.
+// Block = 256 threads; blockIdx.x = work item (bin chunk), blockIdx.y = coil chunk.
+// ---------------------------------------------------------------------------
+template <int NDIM, int WMAX>
+__global__ void __launch_bounds__(256) interp_kernel(
+    Geom g, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
+    const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
+    const float2 *__restrict__ grid, float2 *__restrict__ ksp, int64_t batch,
+    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    using M = Meta<NDIM, WMAX>;
+    const int CC = 1 << cc_log2;
+    const WorkItem it = work[blockIdx.x];
+    const int f = it.bin / g.nbins;
+    int org[3];
+    tile_origin(g, it.bin - f * g.nbins, org);
+    const int R0 = g.T[0] + g.W[0] - 1;
+    const int R1 = NDIM > 1 ? g.T[1] + g.W[1] - 1 : 1;
+    const int R2 = NDIM > 2 ? g.T[2] + g.W[2] - 1 : 1;
+    const int P = R0 * R1 * R2;
+    const int PP = P | 1;
+    float2 *tile = reinterpret_cast<float2 *>(smem);
+    float *wts = reinterpret_cast<float *>(tile + (size_t)CC * PP);
+    int *off = reinterpret_cast<int *>(wts + M::SB * M::NW);
+    int *gi = off + M::SB;
+
+    const int64_t b0 = (int64_t)blockIdx.y * CC;
+    // stage the tile + halo of CC coils (coalesced along x; FFT-order wrap)
+    for (int idx = threadIdx.x; idx < CC * P; idx += blockDim.x) {
+        const int c = idx / P;
+        const int r = idx - c * P;
+        const int rx = r % R0;
+        const int t = r / R0;
+        const int ry = t % R1;
+        const int rz = t / R1;
+        const int64_t b = b0 + c;
+        float2 v = make_float2(0.0f, 0.0f);
+        if (b < batch) {
+            const int px = (org[0] + rx + g.G[0] - g.half[0]) % g.G[0];
+            const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+            const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+            v = grid[(b * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0] + px];
+        }
+        tile[c * PP + r] = v;
+    }
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int spw = 32 >> cc_log2;
+    const int s = lane >> cc_log2;
+    const int c = lane & (CC - 1);
+    const int64_t b = b0 + c;
+    const int Wx = g.W[0], Wy = g.W[1], Wz = g.W[2];
+    
+    for (int base = it.begin; base < it.end; base += M::SB) {
+        const int n = min(M::SB, it.end - base);
+        __syncthreads();  // tile staged / previous batch consumed
+        stage_samples<NDIM, WMAX>(g, org, base, n, sc0, sc1, sc2, sidx, R0, R1, wts, off, gi);
+        __syncthreads();
+        for (int q = warp * spw + s; q < n; q += nwarps * spw) {
+            const float2 acc = gather_taps<NDIM, WMAX>(tile + c * PP + off[q], wts + q * M::NW, Wx, Wy, Wz, R0, R1);
+            const float ar = acc.x, ai = acc.y;
+            if (b < batch) {
+                const int64_t o = b * g.total + gi[q];
+                float2 y = make_float2(ar / scale, ai / scale);
+                if (weight) {
+                    const float wv = weight[wpb ? o : (int64_t)gi[q]];
+                    y.x *= wv;
+                    y.y *= wv;
+                }
+                ksp[o] = y;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float2 load_sample(const void *ksp, int kreal, int64_t o)
+{
+    if (kreal) return make_float2(reinterpret_cast<const float *>(ksp)[o], 0.0f);
+    return reinterpret_cast<const float2 *>(ksp)[o];
+}
+
+// ---------------------------------------------------------------------------
+// Gridding, atomic mode: each block accumulates its bin's samples into a
+// shared-memory tile + halo (shared atomics; lanes of a warp hold distinct
+// coils) and flushes it to the grid with global atomics. The grid must be
+// zeroed first. Summation order across blocks is not fixed.
+// ---------------------------------------------------------------------------
+template <int NDIM, int WMAX>
+__global__ void __launch_bounds__(256) grid_atomic_kernel(
+    Geom g, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
+    const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
+    const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
+    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    using M = Meta<NDIM, WMAX>;
+    const int CC = 1 << cc_log2;
+    const WorkItem it = work[blockIdx.x];
+    const int f = it.bin / g.nbins;
+    int org[3];
+    tile_origin(g, it.bin - f * g.nbins, org);
+    const int R0 = g.T[0] + g.W[0] - 1;
+    const int R1 = NDIM > 1 ? g.T[1] + g.W[1] - 1 : 1;
+    const int R2 = NDIM > 2 ? g.T[2] + g.W[2] - 1 : 1;
+    const int P = R0 * R1 * R2;
+    const int PP = P | 1;
+    float2 *tile = reinterpret_cast<float2 *>(smem);
+    float *wts = reinterpret_cast<float *>(tile + (size_t)CC * PP);
+    int *off = reinterpret_cast<int *>(wts + M::SB * M::NW);
+    int *gi = off + M::SB;
+
+    for (int idx = threadIdx.x; idx < CC * PP; idx += blockDim.x) tile[idx] = make_float2(0.0f, 0.0f);
+
+    const int64_t b0 = (int64_t)blockIdx.y * CC;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const int spw = 32 >> cc_log2;
+    const int s = lane >> cc_log2;
+    const int c = lane & (CC - 1);
+    const int64_t b = b0 + c;
+    const int Wx = g.W[0], Wy = g.W[1], Wz = g.W[2];
+
+    for (int base = it.begin; base < it.end; base += M::SB) {
+        const int n = min(M::SB, it.end - base);
+        __syncthreads();
+        stage_samples<NDIM, WMAX>(g, org, base, n, sc0, sc1, sc2, sidx, R0, R1, wts, off, gi);
+        __syncthreads();
+        for (int q = warp * spw + s; q < n; q += nwarps * spw) {
+            if (b >= batch) continue;
+            const int64_t o = b * g.total + gi[q];
+            float2 v = load_sample(ksp, kreal, o);
+            if (weight) {
+                const float wv = weight[wpb ? o : (int64_t)gi[q]];
+                v.x *= wv;
+                v.y *= wv;
+            }
+            scatter_taps<NDIM, WMAX>(tile + c * PP + off[q], wts + q * M::NW, v, Wx, Wy, Wz, R0, R1);
+        }
+    }
+    __syncthreads();
+    // flush tile + halo with global atomics (FFT-order wrap)
+    for (int idx = threadIdx.x; idx < CC * P; idx += blockDim.x) {
+        const int cc = idx / P;
+        const int r = idx - cc * P;
+        const int64_t bb = b0 + cc;
+        if (bb >= batch) continue;
+        const float2 v = tile[cc * PP + r];
+        if (v.x == 0.0f && v.y == 0.0f) continue;
+        const int rx = r % R0;
+        const int t = r / R0;
+        const int ry = t % R1;
+        const int rz = t / R1;
+        const int px = (org[0] + rx + g.G[0] - g.half[0]) % g.G[0];
+        const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+        const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+        float2 *dst = grid + (bb * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0] + px;
+        atomicAdd(&dst->x, v.x / scale);
+        atomicAdd(&dst->y, v.y / scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gridding, deterministic mode: one warp owns one tile (no halo) for CC coils
+// and visits, in a fixed order, every sample of the bins that can reach the
+// tile (the tile's own bin and its lower neighbours on each axis). Lane
+// (group gr, coil c) owns the tile slices (outermost axis) congruent to gr
+// modulo 32/CC, so every grid value is summed by one lane in sample order:
+// bitwise reproducible, no atomics, and the grid is written exactly once
+// (no zero-fill needed).
+// ---------------------------------------------------------------------------
+constexpr int kOwnerWarps = 2;
+
+template <int NDIM>
+__host__ __device__ inline void owner_dims(const Geom &g, int &slices, int &inner, int &SP, int &CP)
+{
+    slices = g.T[NDIM - 1];
+    inner = 1;
+    for (int a = 0; a < NDIM - 1; a++) inner *= g.T[a];
+    SP = inner | 1;
+    CP = (slices * SP) | 1;
+}
+
+template <int NDIM, int WMAX>
+__global__ void __launch_bounds__(32 * kOwnerWarps) grid_owner_kernel(
+    Geom g, const int32_t *__restrict__ tiles, int ntiles, const int32_t *__restrict__ bin_start,
+    const float *__restrict__ sc0, const float *__restrict__ sc1, const float *__restrict__ sc2,
+    const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal,
+    float2 *__restrict__ grid, int64_t batch, const float *__restrict__ weight, int wpb,
+    float scale, int cc_log2)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CC = 1 << cc_log2;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int u = blockIdx.x * kOwnerWarps + warp;
+    if (u >= ntiles) return;  // warp-uniform; no block-level barriers below
+    int slices, inner, SP, CP;
+    owner_dims<NDIM>(g, slices, inner, SP, CP);
+    constexpr int NW = NDIM * WMAX;
+    float2 *acc = reinterpret_cast<float2 *>(smem) + (size_t)warp * CC * CP;
+    float *wbuf = reinterpret_cast<float *>(reinterpret_cast<float2 *>(smem) + (size_t)kOwnerWarps * CC * CP) +
+                  warp * NW;
+
+    const int key = tiles[u];
+    const int f = key / g.nbins;
+    const int lb = key - f * g.nbins;
+    int org[3], bb[3], Te[3], lo[3], cnt[3];
+    tile_origin(g, lb, org);
+    bb[0] = lb % g.nb[0];
+    bb[1] = (lb / g.nb[0]) % g.nb[1];
+    bb[2] = lb / (g.nb[0] * g.nb[1]);
+    for (int a = 0; a < 3; a++) {
+        Te[a] = min(g.T[a], g.G[a] - org[a]);
+        const int first = pmod(org[a] - g.W[a] + 1, g.G[a]) / g.T[a];
+        lo[a] = first;
+        cnt[a] = pmod(bb[a] - first, g.nb[a]) + 1;
+    }
+    for (int i = lane; i < CC * CP; i += 32) acc[i] = make_float2(0.0f, 0.0f);
+    __syncwarp();
+
+    const int gmask = (1 << (5 - cc_log2)) - 1;  // 32/CC slice groups
+    const int gr = lane >> cc_log2;
+    const int c = lane & (CC - 1);
+    const int64_t b = (int64_t)blockIdx.y * CC + c;
+    const int Wo = g.W[NDIM - 1];
+
+    for (int iz = 0; iz < cnt[2]; iz++)
+        for (int iy = 0; iy < cnt[1]; iy++)
+            for (int ix = 0; ix < cnt[0]; ix++) {
+                const int sb = (((lo[2] + iz) % g.nb[2]) * g.nb[1] + (lo[1] + iy) % g.nb[1]) * g.nb[0] +
+                               (lo[0] + ix) % g.nb[0];
+                const int s0 = bin_start[f * g.nbins + sb];
+                const int s1 = bin_start[f * g.nbins + sb + 1];
+                for (int j = s0; j < s1; j++) {
+                    const float k[3] = {sc0[j], NDIM > 1 ? sc1[j] : 0.0f, NDIM > 2 ? sc2[j] : 0.0f};
+                    int x0[3] = {0, 0, 0}, d[3] = {0, 0, 0};
+                    bool hit = true;
+#pragma unroll
+                    for (int a = 0; a < NDIM; a++) {
+                        x0[a] = first_tap_dev(k[a], g.W[a]);
+                        d[a] = pmod(x0[a], g.G[a]) - org[a];
+                        if (d[a] < 0) d[a] += g.G[a];
+                        hit = hit && (d[a] < Te[a] || d[a] + g.W[a] - 1 >= g.G[a]);
+                    }
+                    if (!hit) continue;  // uniform across the warp
+                    // weights: lane l computes table entries l, l + 32, ...
+                    __syncwarp();  // previous sample's weights fully consumed
+                    for (int e = lane; e < NW; e += 32) {
+                        const int a = e / WMAX, i = e - a * WMAX;
+                        wbuf[e] = i < g.W[a] ? tap_weight(x0[a], i, k[a], g.W[a], g.inv_hw[a], g.beta[a]) : 0.0f;
+                    }
+                    __syncwarp();
+                    if (b >= batch) continue;
+                    const int64_t o = b * g.total + sidx[j];
+                    float2 v = load_sample(ksp, kreal, o);
+                    if (weight) {
+                        const float wv = weight[wpb ? o : (int64_t)sidx[j]];
+                        v.x *= wv;
+                        v.y *= wv;
+                    }
+                    float wx[WMAX];
+#pragma unroll
+                    for (int i = 0; i < WMAX; i++) wx[i] = wbuf[i];
+                    float2 *basep = acc + c * CP;
+                    const int Go = g.G[NDIM - 1];
+                    for (int io = 0; io < Wo; io++) {
+                        int uo = d[NDIM - 1] + io;
+                        if (uo >= Go) uo -= Go;
+                        if (uo >= Te[NDIM - 1] || (uo & gmask) != gr) continue;
+                        float2 *sl = basep + uo * SP;
+                        const float wo = wbuf[(NDIM - 1) * WMAX + io];
+                        if (NDIM == 1) {
+                            sl[0].x += wo * v.x;
+                            sl[0].y += wo * v.y;
+                        } else if (NDIM == 2) {
+#pragma unroll
+                            for (int i = 0; i < WMAX; i++) {
+                                if (i >= g.W[0]) continue;
+                                int ux = d[0] + i;
+                                if (ux >= g.G[0]) ux -= g.G[0];
+                                if (ux >= Te[0]) continue;
+                                const float wv = wo * wx[i];
+                                sl[ux].x += wv * v.x;
+                                sl[ux].y += wv * v.y;
+                            }
+                        } else {
+                            for (int iy2 = 0; iy2 < g.W[1]; iy2++) {
+                                int uy = d[1] + iy2;
+                                if (uy >= g.G[1]) uy -= g.G[1];
+                                if (uy >= Te[1]) continue;
+                                const float wzy = wo * wbuf[WMAX + iy2];
+                                float2 *row = sl + uy * g.T[0];
+#pragma unroll
+                                for (int i = 0; i < WMAX; i++) {
+                                    if (i >= g.W[0]) continue;
+                                    int ux = d[0] + i;
+                                    if (ux >= g.G[0]) ux -= g.G[0];
+                                    if (ux >= Te[0]) continue;
+                                    const float wv = wzy * wx[i];
+                                    row[ux].x += wv * v.x;
+                                    row[ux].y += wv * v.y;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+    __syncwarp();
+    // write the tile interior once, FFT order
+    const int npts = slices * inner;
+    for (int idx = lane; idx < CC * npts; idx += 32) {
+        const int cc = idx / npts;
+        const int r = idx - cc * npts;
+        const int64_t bb2 = (int64_t)blockIdx.y * CC + cc;
+        if (bb2 >= batch) continue;
+        const int so = r / inner;
+        const int ri = r - so * inner;
+        int l[3] = {0, 0, 0};
+        l[NDIM - 1] = so;
+        if (NDIM == 2) l[0] = ri;
+        if (NDIM == 3) {
+            l[0] = ri % g.T[0];
+            l[1] = ri / g.T[0];
+        }
+        if (l[0] >= Te[0] || l[1] >= Te[1] || l[2] >= Te[2]) continue;
+        const float2 v = acc[cc * CP + so * SP + ri];
+        const int px = (org[0] + l[0] + g.G[0] - g.half[0]) % g.G[0];
+        const int py = (org[1] + l[1] + g.G[1] - g.half[1]) % g.G[1];
+        const int pz = (org[2] + l[2] + g.G[2] - g.half[2]) % g.G[2];
+        grid[(bb2 * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0] + px] =
+            make_float2(v.x / scale, v.y / scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int wmax_for(const Geom &g)
+{
+    int w = 1;
+    for (int a = 0; a < g.ndim; a++) w = std::max(w, g.W[a]);
+    if (w <= 2) return 2;
+    if (w <= 4) return 4;
+    if (w <= 8) return 8;
+    return 16;
+}
+
+static size_t region_points(const Geom &g)
+{
+    size_t p = 1;
+    for (int a = 0; a < g.ndim; a++) p *= (size_t)(g.T[a] + g.W[a] - 1);
+    return p | 1;
+}
+
+static int max_smem()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+// Coils per block: a power of two <= 8 covering the batch, reduced until the
+// tile + metadata fit in shared memory.
+static int pick_cc_log2(int64_t batch, size_t per_coil, size_t fixed, size_t limit, int max_log2)
+{
+    int l = 0;
+    while ((1ll << l) < batch && l < max_log2) l++;
+    while (l > 0 && fixed + (per_coil << l) > limit) l--;
+    return l;
+}
+
+template <int NDIM, int WMAX>
+static int launch_interp(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
+                         const float *weight, int wpb, cudaStream_t st)
+{
+    const Geom &g = p->g;
+    using M = Meta<NDIM, WMAX>;
+    const size_t per_coil = region_points(g) * sizeof(float2);
+    const size_t limit = (size_t)max_smem();
+    const int l = pick_cc_log2(batch, per_coil, M::bytes(), limit, 3);
+    const size_t smem = M::bytes() + (per_coil << l);
+    DMR_CHECK(smem <= limit, DMR_ERR_UNSUPPORTED, "interpolation tile needs %zu B of shared memory", smem);
+    auto kern = interp_kernel<NDIM, WMAX>;
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t chunks = ceil_div(batch, 1ll << l);
+    DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+    dim3 grd(p->nwork, (unsigned)chunks);
+    kern<<<grd, 256, smem, st>>>(g, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx,
+                                 grid, ksp, batch, weight, wpb, (float)p->scale, l);
+    DMR_LAUNCHED("interp_kernel");
+    return DMR_OK;
+}
+
+template <int NDIM, int WMAX>
+static int launch_grid(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                       const float *weight, int wpb, int deterministic, cudaStream_t st)
+{
+    const Geom &g = p->g;
+    const size_t limit = (size_t)max_smem();
+    if (!deterministic) {
+        using M = Meta<NDIM, WMAX>;
+        const size_t per_coil = region_points(g) * sizeof(float2);
+        const int l = pick_cc_log2(batch, per_coil, M::bytes(), limit, 3);
+        const size_t smem = M::bytes() + (per_coil << l);
+        DMR_CHECK(smem <= limit, DMR_ERR_UNSUPPORTED, "gridding tile needs %zu B of shared memory", smem);
+        DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * g.nframes * g.gsize * sizeof(float2), st));
+        auto kern = grid_atomic_kernel<NDIM, WMAX>;
+        DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int64_t chunks = ceil_div(batch, 1ll << l);
+        DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+        if (p->nwork == 0) return DMR_OK;
+        dim3 grd(p->nwork, (unsigned)chunks);
+        kern<<<grd, 256, smem, st>>>(g, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx,
+                                     ksp, kreal, grid, batch, weight, wpb, (float)p->scale, l);
+        DMR_LAUNCHED("grid_atomic_kernel");
+        return DMR_OK;
+    }
+    int slices, inner, SP, CP;
+    owner_dims<NDIM>(g, slices, inner, SP, CP);
+    const size_t per_coil = (size_t)CP * sizeof(float2) * kOwnerWarps;
+    const size_t wbytes = (size_t)kOwnerWarps * NDIM * WMAX * sizeof(float);
+    const int l = pick_cc_log2(batch, per_coil, wbytes, limit, 2);
+    const size_t smem = (per_coil << l) + wbytes;
+    DMR_CHECK(smem <= limit, DMR_ERR_UNSUPPORTED, "owner tile needs %zu B of shared memory", smem);
+    auto kern = grid_owner_kernel<NDIM, WMAX>;
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t chunks = ceil_div(batch, 1ll << l);
+    DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+    dim3 grd((unsigned)ceil_div(p->ntiles, kOwnerWarps), (unsigned)chunks);
+    kern<<<grd, 32 * kOwnerWarps, smem, st>>>(g, p->tiles, p->ntiles, p->bin_start, p->scoord[0],
+                                              p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid,
+                                              batch, weight, wpb, (float)p->scale, l);
+    DMR_LAUNCHED("grid_owner_kernel");
+    return DMR_OK;
+}
+
+int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
+                    const float *weight, int wpb, cudaStream_t st)
+{
+    if (p->nwork == 0) return DMR_OK;
+    const int wm = wmax_for(p->g);
+    switch (p->g.ndim * 100 + wm) {
+    case 102: return launch_interp<1, 2>(p, grid, ksp, batch, weight, wpb, st);
+    case 104: return launch_interp<1, 4>(p, grid, ksp, batch, weight, wpb, st);
+    case 108: return launch_interp<1, 8>(p, grid, ksp, batch, weight, wpb, st);
+    case 116: return launch_interp<1, 16>(p, grid, ksp, batch, weight, wpb, st);
+    case 202: return launch_interp<2, 2>(p, grid, ksp, batch, weight, wpb, st);
+    case 204: return launch_interp<2, 4>(p, grid, ksp, batch, weight, wpb, st);
+    case 208: return launch_interp<2, 8>(p, grid, ksp, batch, weight, wpb, st);
+    case 216: return launch_interp<2, 16>(p, grid, ksp, batch, weight, wpb, st);
+    case 302: return launch_interp<3, 2>(p, grid, ksp, batch, weight, wpb, st);
+    case 304: return launch_interp<3, 4>(p, grid, ksp, batch, weight, wpb, st);
+    case 308: return launch_interp<3, 8>(p, grid, ksp, batch, weight, wpb, st);
+    case 316: return launch_interp<3, 16>(p, grid, ksp, batch, weight, wpb, st);
+    default: break;
+    }
+    set_error("unsupported ndim/width");
+    return DMR_ERR_UNSUPPORTED;
+}
+
+int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                  const float *weight, int wpb, int det, cudaStream_t st)
+{
+    const int wm = wmax_for(p->g);
+    switch (p->g.ndim * 100 + wm) {
+    case 102: return launch_grid<1, 2>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 104: return launch_grid<1, 4>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 108: return launch_grid<1, 8>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 116: return launch_grid<1, 16>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 202: return launch_grid<2, 2>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 204: return launch_grid<2, 4>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 208: return launch_grid<2, 8>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 216: return launch_grid<2, 16>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 302: return launch_grid<3, 2>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 304: return launch_grid<3, 4>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 308: return launch_grid<3, 8>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    case 316: return launch_grid<3, 16>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
+    default: break;
+    }
+    set_error("unsupported ndim/width");
+    return DMR_ERR_UNSUPPORTED;
+}
+
+}  // namespace dmr
+
+using namespace dmr;
+
+extern "C" int dmr_interp(const dmr_plan *p, const void *grid, void *kspace, int64_t batch,
+                          const float *weight, int weight_per_batch, void *stream)
+{
+    DMR_CHECK(p && (grid || batch == 0) && (kspace || batch == 0), DMR_ERR_INVALID, "NULL argument");
+    DMR_CHECK(batch >= 0, DMR_ERR_INVALID, "negative batch");
+    if (batch == 0 || p->g.total == 0) return DMR_OK;
+    return interp_dispatch(p, (const float2 *)grid, (float2 *)kspace, batch, weight,
+                           weight_per_batch, (cudaStream_t)stream);
+}
+
+extern "C" int dmr_grid(const dmr_plan *p, const void *kspace, int kspace_real, void *grid,
+                        int64_t batch, const float *weight, int weight_per_batch, int deterministic,
+                        void *stream)
+{
+    DMR_CHECK(p && (grid || batch == 0) && (kspace || batch == 0), DMR_ERR_INVALID, "NULL argument");
+    DMR_CHECK(batch >= 0, DMR_ERR_INVALID, "negative batch");
+    if (batch == 0) return DMR_OK;
+    return grid_dispatch(p, kspace, kspace_real, (float2 *)grid, batch, weight, weight_per_batch,
+                         deterministic, (cudaStream_t)stream);
+}

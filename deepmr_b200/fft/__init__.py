@@ -1,0 +1,51 @@
+"""Non-Cartesian NUFFT on B200 — drop-in for ``deepmr.fft``'s NUFFT API.
+
+One-shot ``nufft`` / ``nufft_adj`` (reference: src/deepmr/fft/__init__.py:145-286)
+and the plan/apply functions of ``deepmr.fft.nufft``.
+"""
+
+from . import nufft as _nufft
+from . import toeplitz as _toeplitz
+from .nufft import (  # noqa: F401
+    NUFFTPlan,
+    apply_nufft,
+    apply_nufft_adj,
+    apply_nufft_selfadj,
+    plan_nufft,
+    plan_toeplitz_nufft,
+)
+from .toeplitz import GramMatrix  # noqa: F401
+
+__all__ = [
+    "nufft",
+    "nufft_adj",
+    "plan_nufft",
+    "apply_nufft",
+    "apply_nufft_adj",
+    "plan_toeplitz_nufft",
+    "apply_nufft_selfadj",
+    "NUFFTPlan",
+    "GramMatrix",
+]
+
+
+def nufft(image, coord, shape=None, basis_adjoint=None, device="cpu", threadsperblock=128,
+          width=4, oversamp=1.25):
+    """N-dimensional NUFFT, plan + apply (reference: src/deepmr/fft/__init__.py:145-218).
+
+    image ``(..., [ncontrasts,] ny, nx)`` or ``(..., [ncontrasts,] nz, ny, nx)``;
+    coord ``(ncontrasts, nviews, nsamples, ndim)`` in grid units, (x, y[, z]).
+    Returns kspace ``(..., [ncontrasts,] nviews, nsamples)`` on the input's device.
+    """
+    ndim = coord.shape[-1] if not isinstance(coord, (list, tuple)) else coord[0].shape[-1]
+    if shape is None:
+        shape = image.shape[-ndim:]
+    plan = _nufft.plan_nufft(coord, shape, width, oversamp, device)
+    return _nufft.apply_nufft(image, plan, basis_adjoint, threadsperblock=threadsperblock)
+
+
+def nufft_adj(kspace, coord, shape, basis=None, device="cpu", threadsperblock=128, width=4,
+              oversamp=1.25):
+    """N-dimensional adjoint NUFFT, plan + apply (reference: src/deepmr/fft/__init__.py:221-286)."""
+    plan = _nufft.plan_nufft(coord, shape, width, oversamp, device)
+    return _nufft.apply_nufft_adj(kspace, plan, basis, threadsperblock=threadsperblock)

@@ -1,0 +1,471 @@
+"""NUFFT plan and application — drop-in for ``deepmr.fft.nufft``.
+
+Same functions, argument meanings, layouts and scale conventions as the
+reference module (src/deepmr/fft/nufft.py); the work runs in the sm_100a CUDA
+library through its C ABI:
+
+* ``plan_nufft``  -> Cartesian-axis test on the device, then a device-resident
+  plan (rescaled coordinates sorted by spatial bin), nufft.py:27-132.
+* ``apply_nufft`` -> one fused apodise/zero-pad/ifftshift kernel, cuFFT, and
+  the bin-tiled interpolation kernel, nufft.py:212-245, 450-528.
+* ``apply_nufft_adj`` -> bin-tiled gridding, cuFFT, one fused
+  fftshift/crop/apodise kernel, nufft.py:289-322, 531-606.
+* ``apply_nufft_selfadj`` -> Toeplitz pad/FFT/multiply/iFFT/crop,
+  nufft.py:351-375, 609-669.
+
+Computation always happens on a CUDA device. ``device="cpu"`` (the reference
+default) keeps its meaning for the *caller*: results are returned on the
+input's device, as the reference does (nufft.py:517-523); the plan computes
+on the current CUDA device.
+"""
+
+__all__ = [
+    "plan_nufft",
+    "plan_toeplitz_nufft",
+    "apply_nufft",
+    "apply_nufft_adj",
+    "apply_nufft_selfadj",
+    "NUFFTPlan",
+]
+
+import ctypes
+import math
+import weakref
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+import torch.autograd as autograd
+
+from .. import _lib
+from . import toeplitz as _toeplitz
+
+# ---------------------------------------------------------------------------
+# device plan
+# ---------------------------------------------------------------------------
+
+
+def compute_device(device):
+    """CUDA device that does the work for a requested ``device``."""
+    _lib.require_cuda()
+    if device is None:
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type == "cuda":
+        return torch.device("cuda", d.index if d.index is not None else torch.cuda.current_device())
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _destroy(handle):
+    try:
+        _lib.lib().dmr_plan_destroy(handle)
+    except Exception:  # interpreter shutdown
+        pass
+
+
+class DevicePlan:
+    """Device-resident interpolator: owns a ``dmr_plan`` of the CUDA library.
+
+    Plays the role of the reference's ``Interpolator`` (src/deepmr/fft/_interp/
+    plan.py:147-187): ``dshape`` is the oversampled grid (z, y, x), ``ishape``
+    the per-frame sample shape (nviews, nsamples), ``scale`` the kernel-sum
+    normalisation.
+    """
+
+    def __init__(self, coord, frame_offsets, ishape, ndim, shape, os_shape, width, beta,
+                 oversamp, device, tile=None):
+        self.ndim = int(ndim)
+        self.dshape = tuple(int(s) for s in os_shape)
+        self.ishape = tuple(int(s) for s in ishape) if ishape is not None else None
+        self.frame_offsets = np.asarray(frame_offsets, dtype=np.int64)
+        self.nframes = len(self.frame_offsets) - 1
+        self.total = int(self.frame_offsets[-1])
+        self.device = device
+        self._params = (shape, os_shape, width, beta, oversamp, tile)
+        self._coord = coord  # raw (total, ndim) float32 on `device`, kept for .to()
+        self._build()
+
+    def _build(self):
+        shape, os_shape, width, beta, oversamp, tile = self._params
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        foff = (ctypes.c_int64 * len(self.frame_offsets))(*self.frame_offsets.tolist())
+        with torch.cuda.device(self.device):
+            _lib.check(
+                L.dmr_plan_create(
+                    self.ndim,
+                    _lib.i32_array(shape),
+                    _lib.i32_array(os_shape),
+                    _lib.i32_array(width),
+                    _lib.f32_array(beta),
+                    _lib.f32_array(oversamp),
+                    _lib.ptr(self._coord),
+                    foff,
+                    self.nframes,
+                    _lib.i32_array(tile) if tile is not None else None,
+                    _lib.stream_ptr(self.device),
+                    ctypes.byref(h),
+                )
+            )
+        self.handle = h
+        sc = ctypes.c_double()
+        _lib.check(L.dmr_plan_scale(h, ctypes.byref(sc)))
+        self.scale = float(sc.value)
+        self._fin = weakref.finalize(self, _destroy, h)
+
+    def to(self, device):
+        dev = compute_device(device)
+        if dev != self.device:
+            self._fin()
+            self.device = dev
+            self._coord = self._coord.to(dev)
+            self._build()
+        return self
+
+    def workspace(self, batch):
+        n = ctypes.c_size_t()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().dmr_nufft_workspace_bytes(self.handle, int(batch), ctypes.byref(n)))
+        return torch.empty(int(n.value), dtype=torch.uint8, device=self.device)
+
+
+@dataclass
+class NUFFTPlan:
+    """NUFFT plan (fields of the reference's NUFFTPlan, nufft.py:379-404)."""
+
+    ndim: int
+    oversamp: tuple
+    width: tuple
+    beta: tuple
+    os_shape: tuple
+    shape: tuple
+    interpolator: object
+    device: str
+
+    def to(self, device):
+        """Dispatch to ``device`` (a CUDA device moves the plan; "cpu" keeps the
+        current CUDA device for compute and only changes where results go)."""
+        if device != self.device:
+            self.interpolator.to(device)
+            self.device = device
+        return self
+
+
+def _axis_param(v, ndim, dtype):
+    if np.isscalar(v):
+        return np.asarray([v] * ndim, dtype=dtype)
+    return np.asarray(v, dtype=dtype)
+
+
+def detect_cartesian(coord_dev, shape_zyx):
+    """Per-axis Cartesian flags in (z, y, x) order (nufft.py:104-109), on the device."""
+    ndim = coord_dev.shape[-1]
+    flags = (ctypes.c_int32 * ndim)()
+    with torch.cuda.device(coord_dev.device):
+        _lib.check(
+            _lib.lib().dmr_detect_cartesian(
+                _lib.ptr(coord_dev), coord_dev.numel() // ndim, ndim,
+                _lib.i32_array([int(s) for s in shape_zyx]), flags, _lib.stream_ptr(coord_dev.device),
+            )
+        )
+    return np.asarray([bool(flags[a]) for a in range(ndim)][::-1])
+
+
+def _frames(coord):
+    """Frames, per-frame sample shape and CSR offsets of a coordinate tensor.
+
+    (ncontrasts, nviews, nsamples, ndim); fewer dims get leading singletons
+    (plan.py:66-77). A list/tuple of per-frame tensors gives frames of uneven
+    length (an extension: samples then lie flat as (..., total)).
+    """
+    if isinstance(coord, (list, tuple)):
+        parts = [torch.as_tensor(c, dtype=torch.float32) for c in coord]
+        ndim = parts[0].shape[-1]
+        lengths = [p.numel() // ndim for p in parts]
+        offs = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int64)
+        flat = torch.cat([p.reshape(-1, ndim) for p in parts], 0)
+        return flat, offs, None, ndim
+    ishape = list(coord.shape[:-1])
+    ndim = coord.shape[-1]
+    while len(ishape) < 3:
+        ishape = [1] + ishape
+    nframes = ishape[0]
+    ishape = ishape[1:]
+    npts = int(np.prod(ishape))
+    offs = (np.arange(nframes + 1, dtype=np.int64) * npts)
+    return coord.reshape(-1, ndim), offs, tuple(ishape), ndim
+
+
+def plan_nufft(coord, shape, width=4, oversamp=1.25, device="cpu", tile=None):
+    """Precompute a NUFFT plan (reference: src/deepmr/fft/nufft.py:27-132).
+
+    Parameters
+    ----------
+    coord : torch.Tensor | list
+        K-space coordinates ``(ncontrasts, nviews, nsamples, ndim)`` in grid
+        units ``(-shape/2, shape/2)``, axis order (x, y[, z]); fewer leading
+        dims are singletons. A list of per-frame coordinate tensors gives frames
+        of uneven length.
+    shape : int | Iterable[int]
+        Image size (z, y, x), scalar for isotropic.
+    width : int | Iterable[int], optional
+        Kaiser-Bessel kernel width. The default is ``4``.
+    oversamp : float | Iterable[float], optional
+        Grid oversampling. The default is ``1.25``.
+    device : str, optional
+        Device of the results for default calls; computation uses CUDA.
+    tile : Iterable[int], optional
+        Spatial bin size (z, y, x); ``None`` uses the tuned default.
+    """
+    dev = compute_device(device)
+    if isinstance(coord, (list, tuple)):
+        flat, offs, ishape, ndim = _frames(coord)
+    else:
+        coord = torch.as_tensor(coord).detach().clone().to(torch.float32)
+        flat, offs, ishape, ndim = _frames(coord)
+    flat = flat.to(dev, torch.float32).contiguous()
+
+    width = _axis_param(width, ndim, np.int16)
+    oversamp = _axis_param(oversamp, ndim, np.float32)
+    # Kaiser-Bessel beta (nufft.py:98), float32 numpy arithmetic
+    beta = math.pi * (((width / oversamp) * (oversamp - 0.5)) ** 2 - 0.8) ** 0.5
+    if np.isscalar(shape):
+        shape = np.asarray([shape] * ndim, dtype=np.int16)
+    else:
+        shape = np.asarray(shape, dtype=np.int16)[-ndim:]
+
+    is_cart = detect_cartesian(flat, shape)
+    oversamp[is_cart] = 1.0
+    width[is_cart] = 1
+    os_shape = np.ceil(oversamp * shape).astype(np.int16)
+
+    interp = DevicePlan(flat, offs, ishape, ndim, shape, os_shape, width, beta, oversamp, dev, tile)
+    return NUFFTPlan(ndim, tuple(oversamp), tuple(width), tuple(beta), tuple(os_shape),
+                     tuple(shape), interp, device)
+
+
+def plan_toeplitz_nufft(coord, shape, basis=None, dcf=None, width=4, device="cpu"):
+    """Toeplitz kernel for the self-adjoint NUFFT (reference: nufft.py:135-168)."""
+    return _toeplitz.plan_toeplitz(coord, shape, basis, dcf, width, device)
+
+
+# ---------------------------------------------------------------------------
+# autograd wrappers (nufft.py:171-348): backward of each operator is the other
+# ---------------------------------------------------------------------------
+class ApplyNUFFT(autograd.Function):
+    @staticmethod
+    def forward(image, nufft_plan, basis_adjoint, weight, device, threadsperblock):
+        return _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblock)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        _, nufft_plan, basis_adjoint, weight, device, threadsperblock = inputs
+        ctx.set_materialize_grads(False)
+        ctx.nufft_plan = nufft_plan
+        ctx.basis_adjoint = basis_adjoint
+        ctx.weight = weight
+        ctx.device = device
+        ctx.threadsperblock = threadsperblock
+
+    @staticmethod
+    def backward(ctx, kspace):
+        basis = ctx.basis_adjoint.conj().t() if ctx.basis_adjoint is not None else None
+        return (
+            _apply_nufft_adj(kspace, ctx.nufft_plan, basis, ctx.weight, ctx.device, ctx.threadsperblock),
+            None, None, None, None, None,
+        )
+
+
+class ApplyNUFFTAdjoint(autograd.Function):
+    @staticmethod
+    def forward(kspace, nufft_plan, basis, weight, device, threadsperblock):
+        return _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        _, nufft_plan, basis, weight, device, threadsperblock = inputs
+        ctx.set_materialize_grads(False)
+        ctx.nufft_plan = nufft_plan
+        ctx.basis = basis
+        ctx.weight = weight
+        ctx.device = device
+        ctx.threadsperblock = threadsperblock
+
+    @staticmethod
+    def backward(ctx, image):
+        basis_adjoint = ctx.basis.conj().t() if ctx.basis is not None else None
+        return (
+            _apply_nufft(image, ctx.nufft_plan, basis_adjoint, ctx.weight, ctx.device, ctx.threadsperblock),
+            None, None, None, None, None,
+        )
+
+
+class ApplyNUFFTSelfAdjoint(autograd.Function):
+    @staticmethod
+    def forward(image, toeplitz_kern, device, threadsperblock):
+        return _apply_nufft_selfadj(image, toeplitz_kern, device, threadsperblock)
+
+    @staticmethod
+    def setup_context(ctx, inputs, output):
+        _, toeplitz_kern, device, threadsperblock = inputs
+        ctx.set_materialize_grads(False)
+        ctx.toeplitz_kern = toeplitz_kern
+        ctx.device = device
+        ctx.threadsperblock = threadsperblock
+
+    @staticmethod
+    def backward(ctx, image):
+        return (_apply_nufft_selfadj(image, ctx.toeplitz_kern, ctx.device, ctx.threadsperblock),
+                None, None, None)
+
+
+def apply_nufft(image, nufft_plan, basis_adjoint=None, weight=None, device=None, threadsperblock=128):
+    """Apply the NUFFT (reference: nufft.py:212-245).
+
+    image ``(..., [ncontrasts,] *shape)`` -> kspace ``(..., [ncontrasts,] nviews, nsamples)``.
+    ``threadsperblock`` is accepted for compatibility and ignored.
+    """
+    return ApplyNUFFT.apply(image, nufft_plan, basis_adjoint, weight, device, threadsperblock)
+
+
+def apply_nufft_adj(kspace, nufft_plan, basis=None, weight=None, device=None, threadsperblock=128):
+    """Apply the adjoint NUFFT (reference: nufft.py:289-322).
+
+    kspace ``(..., [ncontrasts,] nviews, nsamples)`` -> image ``(..., [ncontrasts,] *shape)``.
+    """
+    return ApplyNUFFTAdjoint.apply(kspace, nufft_plan, basis, weight, device, threadsperblock)
+
+
+def apply_nufft_selfadj(image, toeplitz_kern, device=None, threadsperblock=128):
+    """Self-adjoint NUFFT through Toeplitz convolution (reference: nufft.py:351-375)."""
+    return ApplyNUFFTSelfAdjoint.apply(image, toeplitz_kern, device, threadsperblock)
+
+
+# ---------------------------------------------------------------------------
+# implementations
+# ---------------------------------------------------------------------------
+def _as_cfloat(x):
+    x = torch.as_tensor(x)
+    if x.dtype in (torch.float16, torch.float32, torch.float64):
+        return x.to(torch.float32)
+    return x.to(torch.complex64)
+
+
+# Deterministic gridding is the default: it is bitwise reproducible and needs
+# no zero-fill; set to False for the shared-memory atomic variant.
+DETERMINISTIC_GRIDDING = True
+
+
+def _check_basis(basis):
+    if basis is not None:
+        raise NotImplementedError(
+            "low-rank subspace NUFFT (basis / basis_adjoint) is not implemented by deepmr_b200"
+        )
+
+
+def _sample_dims(interp):
+    return len(interp.ishape) if interp.ishape is not None else 1
+
+
+def _sample_shape(interp):
+    return interp.ishape if interp.ishape is not None else (interp.total,)
+
+
+def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
+    """Returns (tensor, per_batch flag) for the C library's weight argument."""
+    if weight is None:
+        return None, 0
+    w = torch.as_tensor(weight, dtype=torch.float32).to(dev)
+    if w.numel() == interp.total:
+        return w.contiguous(), 0
+    full = list(batch_shape) + list(frames_shape) + list(_sample_shape(interp))
+    return torch.broadcast_to(w, full).contiguous(), 1
+
+
+def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblock):
+    isnumpy = isinstance(image, np.ndarray)
+    image = _as_cfloat(image)
+    _check_basis(basis_adjoint)
+    if device is not None:
+        nufft_plan.to(device)
+    interp = nufft_plan.interpolator
+    dev = interp.device
+    ndim = nufft_plan.ndim
+    nframes = interp.nframes
+    odevice = image.device
+    x = image.to(dev)
+    if nframes == 1:
+        batch_shape = x.shape[:-ndim]
+        frames_shape = ()
+    else:
+        batch_shape = x.shape[: -ndim - 1]
+        frames_shape = (nframes,)
+        if x.shape[-ndim - 1] != nframes:
+            raise ValueError(f"expected {nframes} frames before the spatial axes, got {tuple(x.shape)}")
+    if tuple(x.shape[-ndim:]) != tuple(int(s) for s in nufft_plan.shape):
+        raise ValueError(f"image spatial shape {tuple(x.shape[-ndim:])} != plan shape {nufft_plan.shape}")
+    batch = int(np.prod(batch_shape))
+    x = x.contiguous()
+    out = torch.empty(list(batch_shape) + list(frames_shape) + list(_sample_shape(interp)),
+                      dtype=torch.complex64, device=dev)
+    if batch > 0 and interp.total > 0:
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        ws = interp.workspace(batch)
+        with torch.cuda.device(dev):
+            _lib.check(
+                _lib.lib().dmr_nufft_forward(
+                    interp.handle, _lib.ptr(x), int(not x.is_complex()), _lib.ptr(out), batch,
+                    _lib.ptr(w), wpb, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev),
+                )
+            )
+    out = out.to(odevice)
+    return out.numpy(force=True) if isnumpy else out
+
+
+def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock):
+    isnumpy = isinstance(kspace, np.ndarray)
+    kspace = _as_cfloat(kspace)
+    _check_basis(basis)
+    if device is not None:
+        nufft_plan.to(device)
+    interp = nufft_plan.interpolator
+    dev = interp.device
+    ndim = nufft_plan.ndim
+    nframes = interp.nframes
+    odevice = kspace.device
+    y = kspace.to(dev)
+    nsd = _sample_dims(interp)
+    if nframes == 1:
+        batch_shape = y.shape[:-nsd]
+        frames_shape = ()
+    else:
+        batch_shape = y.shape[: -nsd - 1]
+        frames_shape = (nframes,)
+    if tuple(y.shape[len(batch_shape) + len(frames_shape):]) != tuple(_sample_shape(interp)):
+        raise ValueError(f"kspace shape {tuple(y.shape)} does not match the plan samples {_sample_shape(interp)}")
+    batch = int(np.prod(batch_shape))
+    y = y.contiguous()
+    out = torch.empty(list(batch_shape) + list(frames_shape) + [int(s) for s in nufft_plan.shape],
+                      dtype=torch.complex64, device=dev)
+    if batch > 0:
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        ws = interp.workspace(batch)
+        with torch.cuda.device(dev):
+            _lib.check(
+                _lib.lib().dmr_nufft_adjoint(
+                    interp.handle, _lib.ptr(y), int(not y.is_complex()), _lib.ptr(out), batch,
+                    _lib.ptr(w), wpb, int(DETERMINISTIC_GRIDDING), _lib.ptr(ws), ws.numel(),
+                    _lib.stream_ptr(dev),
+                )
+            )
+    out = out.to(odevice)
+    return out.numpy(force=True) if isnumpy else out
+
+
+def _apply_nufft_selfadj(image, toeplitz_kern, device, threadsperblock):
+    isnumpy = isinstance(image, np.ndarray)
+    image = _as_cfloat(image)
+    if device is not None:
+        toeplitz_kern.to(device)
+    out = _toeplitz.apply_toeplitz(image, toeplitz_kern)
+    return out.numpy(force=True) if isnumpy else out

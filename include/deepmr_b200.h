@@ -1,0 +1,196 @@
+/*
+ * deepmr_b200 — C ABI of the B200 (sm_100a) non-Cartesian NUFFT library.
+ *
+ * The entry points replace the kernel seam of the reference NUFFT
+ * (deepmr, src/deepmr/fft/...): the plan builder, the interpolation and
+ * gridding launchers, and the FFT/apodisation/pad/crop steps around them.
+ * Each declaration cites the reference interface it replaces
+ * (paths relative to the reference project).
+ *
+ * Conventions
+ *  - All data pointers are device pointers unless a parameter says "host".
+ *  - complex64 data is interleaved (re, im) float32, i.e. torch.complex64.
+ *  - Spatial shapes and per-axis parameters are given in (z, y, x) order for
+ *    the last `ndim` axes (ndim = 1, 2 or 3); coordinates are (x, y, z)
+ *    along their last axis, in grid units, like the reference.
+ *  - Sample data is laid out (batch, total_samples) where total_samples is
+ *    the sum of the per-frame sample counts (frame f occupies
+ *    [frame_offsets[f], frame_offsets[f+1])). For equal-length frames this is
+ *    exactly the reference's (..., ncontrasts, nviews, nsamples) layout.
+ *  - Images / grids are laid out (batch, nframes, *shape).
+ *  - Every call is ordered on the given CUDA stream (cudaStream_t passed as
+ *    void*); none synchronises the device except dmr_plan_create (which
+ *    reads bin counts back to the host) and dmr_plan_destroy.
+ *  - Return value: 0 on success, a negative DMR_ERR_* code otherwise;
+ *    dmr_last_error() gives a message for the calling host thread.
+ *  - Host-thread safety: distinct plans may be used concurrently; one plan
+ *    may be used from several threads (its FFT handles are locked per call).
+ */
+#ifndef DEEPMR_B200_H
+#define DEEPMR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DMR_OK 0
+#define DMR_ERR_INVALID -1     /* bad argument / shape */
+#define DMR_ERR_CUDA -2        /* CUDA runtime error */
+#define DMR_ERR_OOM -3         /* device allocation failed */
+#define DMR_ERR_COORD -4       /* non-finite coordinate */
+#define DMR_ERR_CUFFT -5       /* cuFFT error */
+#define DMR_ERR_UNSUPPORTED -6 /* configuration not supported */
+#define DMR_ERR_WORKSPACE -7   /* workspace too small */
+
+typedef struct dmr_plan dmr_plan;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int dmr_version(void);
+
+/* Message for the last error raised on this host thread. */
+const char *dmr_last_error(void);
+
+/* Number of kernels this library has launched since load (all threads). */
+int64_t dmr_launch_count(void);
+
+/*
+ * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
+ * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
+ * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the
+ * coordinate axis with the shape entry of the same position). Writes one
+ * flag per coordinate axis to host `is_cart_xyz` (synchronises the stream).
+ */
+int dmr_detect_cartesian(const float *coord, int64_t npts, int ndim,
+                         const int32_t *shape_zyx, int32_t *is_cart_xyz,
+                         void *stream);
+
+/*
+ * Build a device-resident NUFFT plan.
+ * Replaces plan_nufft's interpolator precompute
+ * (src/deepmr/fft/nufft.py:116-122 and src/deepmr/fft/_interp/plan.py:14-143):
+ * instead of materialising (F, M, W) index/value tables per axis, the plan
+ * rescales the coordinates (nufft.py:411-420, float32 multiply then add),
+ * sorts the samples by spatial bin (stable) and keeps the sorted rescaled
+ * coordinates; kernel weights are evaluated inside the gather/scatter kernels.
+ *
+ *  shape, os_shape, width, beta, oversamp: host arrays, (z, y, x) order, the
+ *     values plan_nufft derives (after the Cartesian-axis override: width 1
+ *     and oversamp 1 on Cartesian axes).
+ *  coord: device, (total, ndim) float32, NOT rescaled (grid units).
+ *  frame_offsets: host, nframes+1 int64 CSR offsets into the samples.
+ *  tile: host, (z, y, x) bin size or NULL for the tuned default.
+ */
+int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os_shape,
+                    const int32_t *width, const float *beta,
+                    const float *oversamp, const float *coord,
+                    const int64_t *frame_offsets, int64_t nframes,
+                    const int32_t *tile, void *stream, dmr_plan **out);
+
+/* Free a plan (synchronises the device). */
+int dmr_plan_destroy(dmr_plan *plan);
+
+/* Kernel-sum normalisation of the plan (src/deepmr/fft/_interp/plan.py:190-213). */
+int dmr_plan_scale(const dmr_plan *plan, double *scale);
+
+/* Total samples, frames and the bin tile (z, y, x) chosen by the plan. */
+int dmr_plan_info(const dmr_plan *plan, int64_t *total, int64_t *nframes,
+                  int32_t *tile_zyx);
+
+/*
+ * Interpolation, oversampled grid -> samples, scaled by 1/scale and
+ * multiplied by `weight`.
+ * Replaces do_interpolation[_cuda] + the /scale of apply_interpolation
+ * (src/deepmr/fft/_interp/interp.py:14-120, 651-749) and the weight product
+ * of _apply_nufft (src/deepmr/fft/nufft.py:513-515).
+ *  grid: (batch, nframes, *os_shape) complex64 in FFT order (ifftshifted:
+ *        centred index c is stored at (c - G//2) mod G on every axis),
+ *        i.e. exactly the output of an unshifted cuFFT forward transform.
+ *  kspace: (batch, total) complex64, fully written.
+ *  weight: NULL, (total) float32 if weight_per_batch == 0, or
+ *          (batch, total) float32 if weight_per_batch == 1.
+ */
+int dmr_interp(const dmr_plan *plan, const void *grid, void *kspace,
+               int64_t batch, const float *weight, int weight_per_batch,
+               void *stream);
+
+/*
+ * Gridding, samples -> oversampled grid (FFT order as above), scaled by
+ * 1/scale, after multiplying the samples by `weight`.
+ * Replaces do_gridding[_cuda] + the /scale of apply_gridding
+ * (src/deepmr/fft/_interp/grid.py:14-125, 1026-1168) and the weight product
+ * of _apply_nufft_adj (src/deepmr/fft/nufft.py:577-579).
+ *  kspace: (batch, total) complex64, or float32 if kspace_real == 1.
+ *  grid: (batch, nframes, *os_shape) complex64, fully written.
+ *  deterministic: 0 = shared-memory tiles flushed with global atomics
+ *     (summation order may vary between runs);
+ *     1 = each tile is owned by one warp which sums its contributions in a
+ *     fixed order (bitwise reproducible, no atomics).
+ */
+int dmr_grid(const dmr_plan *plan, const void *kspace, int kspace_real,
+             void *grid, int64_t batch, const float *weight,
+             int weight_per_batch, int deterministic, void *stream);
+
+/* Bytes of workspace the forward/adjoint pipelines need for `batch`. */
+int dmr_nufft_workspace_bytes(dmr_plan *plan, int64_t batch, size_t *bytes);
+
+/*
+ * Forward NUFFT: apodise + zero-pad + ifftshift (one kernel), cuFFT forward,
+ * interpolation (fftshift folded into its indexing) with 1/scale and weight.
+ * Replaces _apply_nufft (src/deepmr/fft/nufft.py:450-528).
+ *  image: (batch, nframes, *shape) complex64, or float32 if image_real == 1.
+ *  kspace: (batch, total) complex64.
+ */
+int dmr_nufft_forward(dmr_plan *plan, const void *image, int image_real,
+                      void *kspace, int64_t batch, const float *weight,
+                      int weight_per_batch, void *workspace,
+                      size_t workspace_bytes, void *stream);
+
+/*
+ * Adjoint NUFFT: gridding (weight, 1/scale, ifftshift folded), cuFFT inverse,
+ * fftshift + crop + 1/G + apodisation (one kernel).
+ * Replaces _apply_nufft_adj (src/deepmr/fft/nufft.py:531-606).
+ *  kspace: (batch, total) complex64, or float32 if kspace_real == 1.
+ *  image: (batch, nframes, *shape) complex64.
+ */
+int dmr_nufft_adjoint(dmr_plan *plan, const void *kspace, int kspace_real,
+                      void *image, int64_t batch, const float *weight,
+                      int weight_per_batch, int deterministic,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* Bytes of workspace dmr_toeplitz_apply / dmr_toeplitz_finalize need. */
+int dmr_toeplitz_workspace_bytes(int ndim, const int32_t *kshape,
+                                 int64_t batch, size_t *bytes);
+
+/*
+ * Toeplitz kernel finalisation of plan_toeplitz
+ * (src/deepmr/fft/toeplitz.py:131-155, plain case): from the point-spread
+ * function psf (nk, *kshape) complex64 computes
+ *   k = ifftshift(fftshift(fftn_ortho(ifftshift(psf)))) / mean(|k| over k != 0)
+ * with NaN replaced by 0, into `kernel` (nk, *kshape).
+ */
+int dmr_toeplitz_finalize(int ndim, const int32_t *kshape, int64_t nk,
+                          const void *psf, void *kernel, void *workspace,
+                          size_t workspace_bytes, void *stream);
+
+/*
+ * Toeplitz self-adjoint: centred zero-pad to kshape, unshifted FFT,
+ * multiply by kernel frame (i mod nk) and by 1/prod(kshape) (the two
+ * orthonormal scalings), unshifted inverse FFT, centred crop.
+ * Replaces _apply_nufft_selfadj (src/deepmr/fft/nufft.py:609-669) with the
+ * plain branch of apply_toeplitz (src/deepmr/fft/_interp/toeplitz.py:84-87).
+ *  image, out: (batch, *ishape) complex64 (or float32 image if image_real);
+ *  batch element i uses kernel frame i mod nk.
+ */
+int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t *ishape,
+                       const void *kernel, int64_t nk, const void *image,
+                       int image_real, void *out, int64_t batch,
+                       void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEEPMR_B200_H */

@@ -1,0 +1,32 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built CUDA library")
+
+
+def golden_cases(prefix=None, kind="nufft"):
+    names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    toep = [n for n in names if n.startswith("toep")]
+    if kind == "toeplitz":
+        return toep
+    return [n for n in names if n not in toep]
+
+
+@pytest.fixture
+def load_golden():
+    import numpy as np
+
+    def _load(name):
+        return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+    return _load

@@ -1,0 +1,179 @@
+"""Generate golden NUFFT vectors by running the reference implementation.
+
+Run in a container where the reference project is available (read-only) at
+``/root/reference``::
+
+    python tests/golden/make_golden.py
+
+The reference's top-level package import needs optional I/O dependencies that
+are absent, so the script registers stub parent packages whose ``__path__``
+points into the reference tree and imports ``deepmr.fft`` directly. Numba's
+cache is redirected to a temporary directory so nothing is written into the
+read-only tree. The CPU Toeplitz path of the reference needs its kernel value
+as a numpy array (src/deepmr/fft/_interp/toeplitz.py:85 calls
+``torch.from_numpy`` on it), so the script converts it after planning.
+
+Each case is saved as ``tests/golden/<name>.npz`` with its inputs, plan
+parameters and the reference outputs. Sizes are kept small (a few hundred KB
+in total) so the fixtures can be committed and the GPU tests can use them on
+machines without the reference.
+"""
+
+import os
+import sys
+import tempfile
+import types
+
+os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="numba_"))
+sys.dont_write_bytecode = True
+
+REF_SRC = "/root/reference/src/deepmr"
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+from deepmr_b200 import synth  # noqa: E402
+
+
+def import_reference():
+    for name, path in [("deepmr", REF_SRC), ("deepmr._signal", REF_SRC + "/_signal")]:
+        mod = types.ModuleType(name)
+        mod.__path__ = [path]
+        sys.modules[name] = mod
+    import deepmr._signal.resize as resize_mod
+
+    sys.modules["deepmr._signal"].resize = resize_mod.resize
+    import deepmr.fft  # noqa: F401
+
+    return sys.modules["deepmr.fft.nufft"], sys.modules["deepmr.fft"]
+
+
+def _np(x):
+    return x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)
+
+
+def nufft_case(N, F, name, coord, shape, batch_shape, width, oversamp, weight=None,
+               real_image=False, real_kspace=False, seed=0):
+    """Run reference forward + adjoint on seeded inputs and save them."""
+    coord = torch.as_tensor(coord, dtype=torch.float32)
+    plan = N.plan_nufft(coord, shape, width=width, oversamp=oversamp)
+    ndim = coord.shape[-1]
+    nframes = coord.shape[0] if coord.ndim == 4 else 1
+    img_shape = list(batch_shape) + ([nframes] if nframes > 1 else []) + list(plan.shape)
+    g = torch.Generator().manual_seed(seed)
+    if real_image:
+        img = torch.randn(img_shape, generator=g, dtype=torch.float32)
+    else:
+        img = torch.complex(torch.randn(img_shape, generator=g), torch.randn(img_shape, generator=g))
+    ksp_shape = list(batch_shape) + ([nframes] if nframes > 1 else []) + list(plan.interpolator.ishape)
+    if real_kspace:
+        ksp = torch.randn(ksp_shape, generator=g, dtype=torch.float32)
+    else:
+        ksp = torch.complex(torch.randn(ksp_shape, generator=g), torch.randn(ksp_shape, generator=g))
+    w = None if weight is None else torch.as_tensor(weight, dtype=torch.float32)
+    y = N.apply_nufft(img.clone(), plan, weight=w)
+    x = N.apply_nufft_adj(ksp.clone(), plan, weight=w)
+    out = dict(
+        coord=_np(coord), shape=np.asarray(shape), width=np.asarray(width),
+        oversamp=np.asarray(oversamp, dtype=np.float64), image=_np(img), kspace=_np(ksp),
+        fwd=_np(y), adj=_np(x), plan_beta=np.asarray(plan.beta, dtype=np.float32),
+        plan_os_shape=np.asarray(plan.os_shape, dtype=np.int32),
+        plan_width=np.asarray(plan.width, dtype=np.int32),
+        plan_oversamp=np.asarray(plan.oversamp, dtype=np.float32),
+        plan_scale=np.float64(plan.interpolator.scale), ndim=np.int32(ndim),
+    )
+    if w is not None:
+        out["weight"] = _np(w)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: fwd {tuple(y.shape)} adj {tuple(x.shape)} os {plan.os_shape} "
+          f"w {plan.width} scale {plan.interpolator.scale:.6g}")
+
+
+def toeplitz_case(N, name, coord, shape, batch_shape, dcf=None, width=4, seed=0):
+    coord = torch.as_tensor(coord, dtype=torch.float32)
+    d = None if dcf is None else torch.as_tensor(dcf, dtype=torch.float32)
+    T = N.plan_toeplitz_nufft(coord, shape, dcf=d, width=width)
+    T.value = T.value.numpy()  # CPU path needs a numpy value (toeplitz.py:85)
+    ndim = coord.shape[-1]
+    nframes = coord.shape[0] if coord.ndim == 4 else 1
+    sh = [shape] * ndim if np.isscalar(shape) else list(shape)
+    img_shape = list(batch_shape) + ([nframes] if nframes > 1 else []) + sh
+    g = torch.Generator().manual_seed(seed)
+    img = torch.complex(torch.randn(img_shape, generator=g), torch.randn(img_shape, generator=g))
+    out_img = N.apply_nufft_selfadj(img.clone(), T)
+    out = dict(coord=_np(coord), shape=np.asarray(shape), width=np.asarray(width),
+               image=_np(img), selfadj=_np(out_img), kernel=np.asarray(T.value),
+               kshape=np.asarray(T.shape, dtype=np.int32), ndim=np.int32(ndim))
+    if d is not None:
+        out["dcf"] = _np(d)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: kernel {np.asarray(T.value).shape} out {tuple(out_img.shape)}")
+
+
+def main():
+    N, _ = import_reference()
+
+    # 2D golden-angle radial, width 3 / oversampling 2 (the 2D benchmark's kernel)
+    c = synth.radial_2d(16, 32, 32)
+    nufft_case(N, None, "radial2d_w3_os2", c, 32, [2], 3, 2.0, weight=synth.ramp_dcf(c))
+
+    # 2D, library defaults width 4 / oversampling 1.25 (grid 30, not a power of 2)
+    c = synth.radial_2d(20, 24, 24, angle_offset=0.1)
+    nufft_case(N, None, "radial2d_w4_os125", c, 24, [3], 4, 1.25)
+
+    # 2D with 3 frames, each with its own rotated trajectory (frames axis before space)
+    c = np.stack([synth.radial_2d(4, 16, 16, angle_offset=0.37 * f) for f in range(3)])
+    nufft_case(N, None, "frames2d", c, 16, [2], 4, 1.25)
+
+    # 2D odd/anisotropic matrix (15, 20) and odd oversampled grid; real-valued inputs
+    c = synth.radial_2d(12, 20, (15, 20), angle_offset=0.2)
+    nufft_case(N, None, "aniso2d_real", c, (15, 20), [2], 3, 1.25,
+               real_image=True, real_kspace=True)
+
+    # 2D edge coordinates: exact -N/2, +N/2 (wraps), half-integers where k - W/2 is integral
+    rng = np.random.default_rng(5)
+    c = rng.uniform(-8, 8, size=(3, 10, 2)).astype(np.float32)
+    c[0, 0] = [-8.0, -8.0]
+    c[0, 1] = [8.0, 7.5]
+    c[0, 2] = [0.5, -0.5]
+    c[0, 3] = [1.5, 2.25]
+    c[1, 4] = [-7.9999995, 7.9999995]
+    nufft_case(N, None, "edges2d", c, 16, [1], 4, 1.25, weight=rng.uniform(0.1, 1, (3, 10)))
+
+    # 1D
+    c = np.sort(rng.uniform(-16, 16, size=(1, 40, 1)).astype(np.float32), axis=1)
+    nufft_case(N, None, "line1d", c, 32, [2], 4, 1.25)
+
+    # 3D golden-means kooshball, width 4 / oversampling 1.25 (the 3D benchmark's kernel)
+    c = synth.kooshball_3d(40, 16, 12)
+    nufft_case(N, None, "koosh3d_w4_os125", c, 12, [2], 4, 1.25, weight=synth.ramp_dcf(c))
+
+    # 3D anisotropic matrix, per-axis widths and oversampling
+    c = synth.kooshball_3d(30, 12, (8, 10, 12))
+    nufft_case(N, None, "aniso3d", c, (8, 10, 12), [1], (3, 4, 5), (1.5, 1.25, 2.0))
+
+    # Cartesian bypass: integer coordinates (every axis detected Cartesian, W=1)
+    nodes = np.arange(6) - 3
+    yy, xx = np.meshgrid(nodes, nodes, indexing="ij")
+    c = np.stack([xx.ravel(), yy.ravel()], -1)[None].astype(np.float32)
+    nufft_case(N, None, "cart2d", c, 6, [2], 4, 1.25)
+
+    # Mixed: x Cartesian (integers), y non-Cartesian
+    c = np.stack([np.repeat(np.arange(-4, 4), 5), rng.uniform(-4, 4, 40)], -1)[None].astype(np.float32)
+    nufft_case(N, None, "mixed2d", c, 8, [2], 4, 1.25)
+
+    # Toeplitz self-adjoint, 2D and 3D, with and without density weights, with frames
+    c = synth.radial_2d(24, 32, 16)
+    toeplitz_case(N, "toep2d", c, 16, [2], dcf=synth.ramp_dcf(c))
+    c = synth.radial_2d(10, 16, 12, angle_offset=0.3)
+    toeplitz_case(N, "toep2d_nodcf", c, 12, [1])
+    c = np.stack([synth.radial_2d(6, 16, 10, angle_offset=0.5 * f) for f in range(2)])
+    toeplitz_case(N, "toep2d_frames", c, 10, [2])
+    c = synth.kooshball_3d(30, 16, 8)
+    toeplitz_case(N, "toep3d", c, 8, [2], dcf=synth.ramp_dcf(c))
+
+
+if __name__ == "__main__":
+    main()
