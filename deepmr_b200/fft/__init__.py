@@ -26,7 +26,27 @@ __all__ = [
     "apply_nufft_selfadj",
     "NUFFTPlan",
     "GramMatrix",
+    "set_deterministic_gridding",
+    "deterministic_gridding",
 ]
+
+
+def set_deterministic_gridding(flag=True):
+    """Select the gridding kernel used by the adjoint NUFFT.
+
+    True (default): each grid tile is summed by one warp in a fixed sample
+    order — bitwise reproducible. False: shared-memory tiles flushed with
+    global atomics (summation order may vary between runs).
+    Returns the previous setting.
+    """
+    old = _nufft.DETERMINISTIC_GRIDDING
+    _nufft.DETERMINISTIC_GRIDDING = bool(flag)
+    return old
+
+
+def deterministic_gridding():
+    """Current gridding mode (see set_deterministic_gridding)."""
+    return _nufft.DETERMINISTIC_GRIDDING
 
 
 def nufft(image, coord, shape=None, basis_adjoint=None, device="cpu", threadsperblock=128,

@@ -344,6 +344,18 @@ def apply_nufft_selfadj(image, toeplitz_kern, device=None, threadsperblock=128):
 # ---------------------------------------------------------------------------
 # implementations
 # ---------------------------------------------------------------------------
+def _to_origin(out, like):
+    """Return ``out`` on the device of ``like``; pinned CPU inputs get pinned outputs
+    (so the device-to-host copy runs at full PCIe speed)."""
+    if like.device == out.device:
+        return out
+    if like.device.type == "cpu" and like.is_pinned():
+        host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+        host.copy_(out)
+        return host
+    return out.to(like.device)
+
+
 def _as_cfloat(x):
     x = torch.as_tensor(x)
     if x.dtype in (torch.float16, torch.float32, torch.float64):
@@ -392,7 +404,6 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
     dev = interp.device
     ndim = nufft_plan.ndim
     nframes = interp.nframes
-    odevice = image.device
     x = image.to(dev)
     if nframes == 1:
         batch_shape = x.shape[:-ndim]
@@ -418,7 +429,7 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
                     _lib.ptr(w), wpb, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev),
                 )
             )
-    out = out.to(odevice)
+    out = _to_origin(out, image)
     return out.numpy(force=True) if isnumpy else out
 
 
@@ -432,7 +443,6 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock)
     dev = interp.device
     ndim = nufft_plan.ndim
     nframes = interp.nframes
-    odevice = kspace.device
     y = kspace.to(dev)
     nsd = _sample_dims(interp)
     if nframes == 1:
@@ -458,7 +468,7 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock)
                     _lib.stream_ptr(dev),
                 )
             )
-    out = out.to(odevice)
+    out = _to_origin(out, kspace)
     return out.numpy(force=True) if isnumpy else out
 
 

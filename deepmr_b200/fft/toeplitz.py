@@ -103,7 +103,6 @@ def apply_toeplitz(image, toeplitz_kernel):
     dev = kval.device
     if dev.type != "cuda":
         raise RuntimeError("Toeplitz kernel must live on a CUDA device")
-    odevice = image.device
     x = image.to(dev).contiguous()
     ishape = [int(s) for s in x.shape[-ndim:]]
     K = [int(k) for k in toeplitz_kernel.shape]
@@ -120,4 +119,6 @@ def apply_toeplitz(image, toeplitz_kernel):
                 ndim, _lib.i32_array(K), _lib.i32_array(ishape), _lib.ptr(kv), nk, _lib.ptr(x),
                 int(not x.is_complex()), _lib.ptr(out), batch, _lib.ptr(ws), ws.numel(),
                 _lib.stream_ptr(dev)))
-    return out.to(odevice)
+    from .nufft import _to_origin
+
+    return _to_origin(out, image)

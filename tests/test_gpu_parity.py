@@ -38,12 +38,11 @@ def F():
 
 @pytest.fixture(params=[True, False], ids=["det", "atomic"])
 def grid_mode(request):
-    from deepmr_b200.fft import nufft as N
+    import deepmr_b200.fft as F
 
-    old = N.DETERMINISTIC_GRIDDING
-    N.DETERMINISTIC_GRIDDING = request.param
+    old = F.set_deterministic_gridding(request.param)
     yield request.param
-    N.DETERMINISTIC_GRIDDING = old
+    F.set_deterministic_gridding(old)
 
 
 @pytest.mark.parametrize("name", golden_cases())
