@@ -49,13 +49,15 @@ def _workspace(ndim, kshape, batch, dev):
 
 def plan_toeplitz(coord, shape, basis=None, dcf=None, width=6, device="cpu"):
     """Compute the Toeplitz kernel of A^H A (reference: toeplitz.py:15-157)."""
-    from . import nufft as _nufft  # deferred: nufft imports this module
+    # deferred import (nufft imports this module); import names from the
+    # submodule: the package attribute `nufft` is the one-shot function
+    from .nufft import apply_nufft_adj, compute_device, detect_cartesian, plan_nufft
 
     if basis is not None:
         raise NotImplementedError(
             "low-rank subspace Toeplitz (basis) is not implemented by deepmr_b200"
         )
-    dev = _nufft.compute_device(device)
+    dev = compute_device(device)
     coord = torch.as_tensor(coord, dtype=torch.float32)
     ndim = coord.shape[-1]
     oversamp = np.asarray([2.0] * ndim)
@@ -69,15 +71,15 @@ def plan_toeplitz(coord, shape, basis=None, dcf=None, width=6, device="cpu"):
         dcf = torch.as_tensor(dcf).to(dev)
     delta = torch.ones(list(coord.shape[:-1]), dtype=torch.float32, device=dev)
 
-    is_cart = _nufft.detect_cartesian(coord.reshape(-1, ndim).to(dev).contiguous(), shape)
+    is_cart = detect_cartesian(coord.reshape(-1, ndim).to(dev).contiguous(), shape)
     oversamp[is_cart] = 1.0
     kshape = np.ceil(oversamp * shape).astype(np.int16)
 
     # point-spread function on the 2x grid (toeplitz.py:122-129); the plan casts
     # the float64 product back to float32
     coord2 = coord * torch.as_tensor(oversamp)
-    plan = _nufft.plan_nufft(coord2, kshape, width, 1.25, dev)
-    psf = _nufft.apply_nufft_adj(dcf * delta, plan)
+    plan = plan_nufft(coord2, kshape, width, 1.25, dev)
+    psf = apply_nufft_adj(dcf * delta, plan)
     psf = psf.to(dev).contiguous()
 
     K = [int(k) for k in kshape]

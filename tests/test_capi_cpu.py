@@ -95,3 +95,22 @@ def test_synthetic_generators_are_seeded():
     assert torch.equal(x, synth.complex_gaussian((3, 4), seed=1))
     m = synth.coil_maps(4, (8, 8), seed=0)
     np.testing.assert_allclose((np.abs(m) ** 2).sum(0), 1.0, rtol=1e-5)
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_public_api_fails_loudly_without_cuda():
+    """Every entry point reaches the CUDA requirement and raises (no CPU fallback)."""
+    import deepmr_b200.fft as F
+
+    c = torch.zeros(1, 4, 2)
+    img = torch.zeros(2, 8, 8, dtype=torch.complex64)
+    calls = [
+        lambda: F.plan_nufft(c, 8),
+        lambda: F.nufft(img, c),
+        lambda: F.nufft_adj(torch.zeros(2, 1, 4, dtype=torch.complex64), c, 8),
+        lambda: F.plan_toeplitz_nufft(c, 8),
+        lambda: F.plan_toeplitz_nufft(c, 8, dcf=torch.ones(1, 4)),
+    ]
+    for call in calls:
+        with pytest.raises(RuntimeError, match="CUDA"):
+            call()
