@@ -34,8 +34,8 @@ __all__ = [
 def set_deterministic_gridding(flag=True):
     """Select the gridding kernel used by the adjoint NUFFT.
 
-    True (default): each grid tile is summed by one warp in a fixed sample
-    order — bitwise reproducible. False: shared-memory tiles flushed with
+    True: each grid tile is summed by one warp in a fixed sample order —
+    bitwise reproducible. False (default): shared-memory tiles flushed with
     global atomics (summation order may vary between runs).
     Returns the previous setting.
     """

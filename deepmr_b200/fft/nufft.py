@@ -363,9 +363,9 @@ def _as_cfloat(x):
     return x.to(torch.complex64)
 
 
-# Deterministic gridding is the default: it is bitwise reproducible and needs
-# no zero-fill; set to False for the shared-memory atomic variant.
-DETERMINISTIC_GRIDDING = True
+# Gridding kernel of the adjoint: False (default) = shared-memory tiles flushed
+# with global atomics; True = fixed-order owner tiles (bitwise reproducible).
+DETERMINISTIC_GRIDDING = False
 
 
 def _check_basis(basis):
