@@ -1,5 +1,5 @@
 // NUFFT plan construction on the device: Cartesian-axis test, coordinate
-// rescale, spatial binning and a stable sort of the samples by bin.
+// rescale, spatial binning and a stable sort of the samples by (bin, cell).
 //
 // Reference: plan_nufft (src/deepmr/fft/nufft.py:27-132) and
 // plan_interpolator (src/deepmr/fft/_interp/plan.py:14-143). The reference
@@ -79,7 +79,7 @@ __global__ void preprocess_kernel(Geom g, const float *__restrict__ coord,
             const int mid = (lo + hi) >> 1;
             if (foff[mid] <= i) lo = mid; else hi = mid;
         }
-        int b[3] = {0, 0, 0};
+        int b[3] = {0, 0, 0}, l[3] = {0, 0, 0};
         for (int a = 0; a < g.ndim; a++) {
             float k = __fadd_rn(__fmul_rn(coord[i * g.ndim + a], sc[a]), sh[a]);
             if (!(fabsf(k) < 1.0e8f)) {  // non-finite or absurd coordinate
@@ -87,12 +87,16 @@ __global__ void preprocess_kernel(Geom g, const float *__restrict__ coord,
                 k = 0.0f;
             }
             rk[a][i] = k;
-            b[a] = pmod(first_tap(k, g.W[a]), g.G[a]) / g.T[a];
+            const int x0m = pmod(first_tap(k, g.W[a]), g.G[a]);
+            b[a] = x0m / g.T[a];
+            l[a] = x0m - b[a] * g.T[a];
         }
-        const int key = lo * g.nbins + (b[2] * g.nb[1] + b[1]) * g.nb[0] + b[0];
-        keys[i] = key;
+        // sort key: (frame, bin, cell of the first tap inside the bin)
+        const int bin = lo * g.nbins + (b[2] * g.nb[1] + b[1]) * g.nb[0] + b[0];
+        const int cell = (l[2] * g.T[1] + l[1]) * g.T[0] + l[0];
+        keys[i] = bin * (g.T[0] * g.T[1] * g.T[2]) + cell;
         vals[i] = (int32_t)i;
-        atomicAdd(&counts[key], 1);
+        atomicAdd(&counts[bin], 1);
     }
 }
 
@@ -298,7 +302,8 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     g.nbins = g.nb[0] * g.nb[1] * g.nb[2];
     g.gsize = (int64_t)g.G[0] * g.G[1] * g.G[2];
     g.isize = (int64_t)g.N[0] * g.N[1] * g.N[2];
-    DMR_CHECK((int64_t)g.nbins * nframes < INT32_MAX, DMR_ERR_UNSUPPORTED, "too many bins");
+    DMR_CHECK((int64_t)g.nbins * nframes * g.T[0] * g.T[1] * g.T[2] < INT32_MAX, DMR_ERR_UNSUPPORTED,
+              "too many bins x cells for 32-bit sort keys");
     p->scale = kernel_scale(g);
     p->frame_offsets.assign(frame_offsets, frame_offsets + nframes + 1);
 
@@ -353,8 +358,9 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
             g, coord, d_foff, sc[0], sc[1], sc[2], sh[0], sh[1], sh[2], rk[0], rk[1], rk[2],
             keys, vals, counts, d_err);
         DMR_LAUNCHED("preprocess_kernel");
+        const int64_t nsort = nkeys * (int64_t)g.T[0] * g.T[1] * g.T[2];
         int end_bit = 1;
-        while ((1ll << end_bit) < nkeys) end_bit++;
+        while ((1ll << end_bit) < nsort) end_bit++;
         size_t temp_bytes = 0;
         DMR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys_s, vals, p->sidx,
                                                  (int)total, 0, end_bit, st));

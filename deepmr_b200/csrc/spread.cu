@@ -340,6 +340,298 @@ __global__ void __launch_bounds__(256) grid_atomic_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// Cell-cube kernels. Samples are sorted by (bin, cell of their first tap), and
+// in the kooshball / radial centre thousands of samples share a cell, so the
+// W^NDIM taps of a cell are held in registers and reused across the cell's
+// samples: interpolation reads the cube from the shared tile once per cell,
+// gridding accumulates into the cube and flushes it once per cell.
+//
+// Lane layout: lane = (stream s, slice g, coil c). A lane owns slice g of the
+// cube (one tap index along the outermost axis: z in 3D, y in 2D, x in 1D) for
+// coil c; NG = next power of two >= W slices, CC coils, NS = 32/(NG*CC)
+// independent sample streams per warp. Interpolation reduces the NG slice
+// partial sums with warp shuffles. Complex arithmetic uses the packed FP32
+// instructions (__ffma2_rn / __fmul2_rn).
+// ---------------------------------------------------------------------------
+template <int W>
+struct SliceGroups {
+    static constexpr int value = W <= 1 ? 1 : (W <= 2 ? 2 : (W <= 4 ? 4 : (W <= 8 ? 8 : 16)));
+};
+
+// shared-memory geometry of the staged tile + halo for one coil chunk
+struct Region {
+    int R0, R1, R2;  // extents with halo (T + W - 1 on used axes)
+    int SP;          // slice pitch of the outermost axis (padded against bank conflicts)
+    int PP;          // coil pitch (padded)
+};
+
+template <int NDIM, int W>
+struct CubeShape {
+    static constexpr int NG = SliceGroups<W>::value;
+    static constexpr int IN = NDIM == 3 ? W * W : (NDIM == 2 ? W : 1);  // taps per slice
+    static constexpr int NW = NDIM * W;                                  // staged weights
+    static constexpr int SB = NW <= 16 ? 256 : (NW <= 32 ? 128 : 64);    // staged samples
+    static size_t meta_bytes() { return (size_t)SB * (NW * sizeof(float) + 2 * sizeof(int)); }
+};
+
+template <int NDIM, int W>
+__device__ __forceinline__ int inner_off(int j, int R0)
+{
+    if (NDIM == 3) return (j / W) * R0 + (j % W);
+    if (NDIM == 2) return j;
+    return 0;
+}
+
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+
+// stage weights (zero beyond an axis' own width), first-tap offset in the
+// region, and global index of samples [base, base + n)
+template <int NDIM, int W>
+__device__ __forceinline__ void stage_cube_samples(const Geom &g, const int org[3], const Region &rg,
+                                                   int base, int n, const float *__restrict__ sc0,
+                                                   const float *__restrict__ sc1,
+                                                   const float *__restrict__ sc2,
+                                                   const int32_t *__restrict__ sidx, float *wts,
+                                                   int *off, int *gi)
+{
+    constexpr int NW = NDIM * W;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const int j = base + t;
+        const float k[3] = {sc0[j], NDIM > 1 ? sc1[j] : 0.0f, NDIM > 2 ? sc2[j] : 0.0f};
+        int l[3] = {0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < NDIM; a++) {
+            const int x0 = first_tap_dev(k[a], g.W[a]);
+            l[a] = pmod(x0, g.G[a]) - org[a];
+#pragma unroll
+            for (int i = 0; i < W; i++)
+                wts[t * NW + a * W + i] =
+                    i < g.W[a] ? tap_weight(x0, i, k[a], g.W[a], g.inv_hw[a], g.beta[a]) : 0.0f;
+        }
+        off[t] = NDIM == 3 ? l[2] * rg.SP + l[1] * rg.R0 + l[0] : (NDIM == 2 ? l[1] * rg.SP + l[0] : l[0]);
+        gi[t] = sidx[j];
+    }
+}
+
+// stage (or, with `flush`, atomically add back) the tile + halo of CC coils
+template <int NDIM>
+__device__ __forceinline__ void region_io(const Geom &g, const Region &rg, const int org[3], int f,
+                                          int64_t b0, int CC, int64_t batch, float2 *tile,
+                                          float2 *__restrict__ grid, bool flush, float scale)
+{
+    const int rows = rg.R1 * rg.R2;
+    const int per = rows * rg.R0;
+    for (int e = threadIdx.x; e < CC * per; e += blockDim.x) {
+        const int c = e / per;
+        const int r = e - c * per;
+        const int row = r / rg.R0;
+        const int rx = r - row * rg.R0;
+        const int ry = row % rg.R1;
+        const int rz = row / rg.R1;
+        const int si = c * rg.PP + (NDIM == 3 ? rz * rg.SP + ry * rg.R0 + rx : (NDIM == 2 ? ry * rg.SP + rx : rx));
+        const int64_t b = b0 + c;
+        if (b >= batch) {
+            if (!flush) tile[si] = make_float2(0.0f, 0.0f);
+            continue;
+        }
+        const int px = (org[0] + rx + g.G[0] - g.half[0]) % g.G[0];
+        const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+        const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+        float2 *gp = grid + (b * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0] + px;
+        if (!flush) {
+            tile[si] = *gp;
+        } else {
+            const float2 v = tile[si];
+            if (v.x != 0.0f || v.y != 0.0f) atomicAdd(gp, make_float2(v.x / scale, v.y / scale));
+        }
+    }
+}
+
+template <int NDIM, int W>
+__global__ void __launch_bounds__(256) interp_cube_kernel(
+    Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
+    const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
+    const float2 *__restrict__ grid, float2 *__restrict__ ksp, int64_t batch,
+    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+{
+    using S = CubeShape<NDIM, W>;
+    constexpr int NG = S::NG, IN = S::IN, NW = S::NW;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CC = 1 << cc_log2;
+    const WorkItem it = work[blockIdx.x];
+    const int f = it.bin / g.nbins;
+    int org[3];
+    tile_origin(g, it.bin - f * g.nbins, org);
+    float2 *tile = reinterpret_cast<float2 *>(smem);
+    float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
+    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *gi = off + S::SB;
+    const int64_t b0 = (int64_t)blockIdx.y * CC;
+    region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, const_cast<float2 *>(grid), false, 1.0f);
+
+    const int lane = threadIdx.x & 31;
+    const int c = lane & (CC - 1);
+    const int gs = (lane >> cc_log2) & (NG - 1);
+    const int s = lane / (CC * NG);
+    const int ns = 32 / (CC * NG);
+    const int stream = (threadIdx.x >> 5) * ns + s;
+    const int nstreams = (blockDim.x >> 5) * ns;
+    const unsigned smask = (CC * NG == 32) ? 0xffffffffu : (((1u << (CC * NG)) - 1u) << (s * CC * NG));
+    const int64_t b = b0 + c;
+
+    for (int base = it.begin; base < it.end; base += S::SB) {
+        const int n = min(S::SB, it.end - base);
+        __syncthreads();
+        stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
+        __syncthreads();
+        const int q0 = (int)((int64_t)n * stream / nstreams);
+        const int q1 = (int)((int64_t)n * (stream + 1) / nstreams);
+        int cur = -1;
+        float2 cube[IN];
+#pragma unroll
+        for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+        for (int q = q0; q < q1; q++) {
+            const int o = off[q];
+            if (o != cur) {
+                cur = o;
+                if (gs < W) {
+                    const float2 *src = tile + c * rg.PP + o + gs * rg.SP;
+#pragma unroll
+                    for (int j = 0; j < IN; j++) cube[j] = src[inner_off<NDIM, W>(j, rg.R0)];
+                }
+            }
+            const float *w = wts + q * NW;
+            float2 acc = make_float2(0.0f, 0.0f);
+            if (NDIM == 3) {
+#pragma unroll
+                for (int jy = 0; jy < W; jy++) {
+                    float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (int ix = 0; ix < W; ix++) r = __ffma2_rn(f2(w[ix]), cube[jy * W + ix], r);
+                    acc = __ffma2_rn(f2(w[W + jy]), r, acc);
+                }
+            } else if (NDIM == 2) {
+#pragma unroll
+                for (int ix = 0; ix < W; ix++) acc = __ffma2_rn(f2(w[ix]), cube[ix], acc);
+            } else {
+                acc = cube[0];
+            }
+            const float wo = gs < W ? w[(NDIM - 1) * W + gs] : 0.0f;
+            acc = __fmul2_rn(f2(wo), acc);
+#pragma unroll
+            for (int m = 1; m < NG; m <<= 1) {
+                acc.x += __shfl_xor_sync(smask, acc.x, m * CC);
+                acc.y += __shfl_xor_sync(smask, acc.y, m * CC);
+            }
+            if (gs == 0 && b < batch) {
+                const int64_t o2 = b * g.total + gi[q];
+                float2 y = make_float2(acc.x / scale, acc.y / scale);
+                if (weight) {
+                    const float wv = weight[wpb ? o2 : (int64_t)gi[q]];
+                    y.x *= wv;
+                    y.y *= wv;
+                }
+                ksp[o2] = y;
+            }
+        }
+    }
+}
+
+template <int NDIM, int W>
+__device__ __forceinline__ void flush_cube(float2 *dst, const float2 *cube, int R0)
+{
+    constexpr int IN = CubeShape<NDIM, W>::IN;
+#pragma unroll
+    for (int j = 0; j < IN; j++) {
+        float2 *p = dst + inner_off<NDIM, W>(j, R0);
+        atomicAdd(&p->x, cube[j].x);
+        atomicAdd(&p->y, cube[j].y);
+    }
+}
+
+template <int NDIM, int W>
+__global__ void __launch_bounds__(256) grid_cube_kernel(
+    Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
+    const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
+    const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
+    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+{
+    using S = CubeShape<NDIM, W>;
+    constexpr int NG = S::NG, IN = S::IN, NW = S::NW;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CC = 1 << cc_log2;
+    const WorkItem it = work[blockIdx.x];
+    const int f = it.bin / g.nbins;
+    int org[3];
+    tile_origin(g, it.bin - f * g.nbins, org);
+    float2 *tile = reinterpret_cast<float2 *>(smem);
+    float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
+    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *gi = off + S::SB;
+    for (int e = threadIdx.x; e < CC * rg.PP; e += blockDim.x) tile[e] = make_float2(0.0f, 0.0f);
+    const int64_t b0 = (int64_t)blockIdx.y * CC;
+
+    const int lane = threadIdx.x & 31;
+    const int c = lane & (CC - 1);
+    const int gs = (lane >> cc_log2) & (NG - 1);
+    const int s = lane / (CC * NG);
+    const int ns = 32 / (CC * NG);
+    const int stream = (threadIdx.x >> 5) * ns + s;
+    const int nstreams = (blockDim.x >> 5) * ns;
+    const int64_t b = b0 + c;
+    const bool active = gs < W && b < batch;
+
+    for (int base = it.begin; base < it.end; base += S::SB) {
+        const int n = min(S::SB, it.end - base);
+        __syncthreads();
+        stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
+        __syncthreads();
+        const int q0 = (int)((int64_t)n * stream / nstreams);
+        const int q1 = (int)((int64_t)n * (stream + 1) / nstreams);
+        int cur = -1;
+        float2 cube[IN];
+#pragma unroll
+        for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+        for (int q = q0; q < q1; q++) {
+            const int o = off[q];
+            if (o != cur) {
+                if (cur >= 0 && active) flush_cube<NDIM, W>(tile + c * rg.PP + cur + gs * rg.SP, cube, rg.R0);
+#pragma unroll
+                for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+                cur = o;
+            }
+            if (!active) continue;
+            const int64_t o2 = b * g.total + gi[q];
+            float2 v = load_sample(ksp, kreal, o2);
+            if (weight) {
+                const float wv = weight[wpb ? o2 : (int64_t)gi[q]];
+                v.x *= wv;
+                v.y *= wv;
+            }
+            const float *w = wts + q * NW;
+            const float2 u = __fmul2_rn(f2(w[(NDIM - 1) * W + gs]), v);
+            if (NDIM == 3) {
+#pragma unroll
+                for (int jy = 0; jy < W; jy++) {
+                    const float2 t = __fmul2_rn(f2(w[W + jy]), u);
+#pragma unroll
+                    for (int ix = 0; ix < W; ix++) cube[jy * W + ix] = __ffma2_rn(f2(w[ix]), t, cube[jy * W + ix]);
+                }
+            } else if (NDIM == 2) {
+#pragma unroll
+                for (int ix = 0; ix < W; ix++) cube[ix] = __ffma2_rn(f2(w[ix]), u, cube[ix]);
+            } else {
+                cube[0].x += u.x;
+                cube[0].y += u.y;
+            }
+        }
+        if (cur >= 0 && active) flush_cube<NDIM, W>(tile + c * rg.PP + cur + gs * rg.SP, cube, rg.R0);
+    }
+    __syncthreads();
+    region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, scale);
+}
+
+// ---------------------------------------------------------------------------
 // Gridding, deterministic mode: one warp owns one tile (no halo) for CC coils
 // and visits, in a fixed order, every sample of the bins that can reach the
 // tile (the tile's own bin and its lower neighbours on each axis). Lane
@@ -615,10 +907,144 @@ static int launch_grid(const dmr_plan *p, const void *ksp, int kreal, float2 *gr
     return DMR_OK;
 }
 
+// ---- cell-cube launchers ----------------------------------------------------
+static int pad_mod16(int x, int m)
+{
+    m &= 15;
+    return x + (((m - x) % 16) + 16) % 16;
+}
+
+template <int NDIM, int W>
+static Region cube_region(const Geom &g, int CC)
+{
+    Region r;
+    r.R0 = g.T[0] + W - 1;
+    r.R1 = NDIM > 1 ? g.T[1] + W - 1 : 1;
+    r.R2 = NDIM > 2 ? g.T[2] + W - 1 : 1;
+    int P;
+    if (NDIM == 3) {
+        r.SP = pad_mod16(r.R0 * r.R1, CC);
+        P = r.SP * r.R2;
+    } else if (NDIM == 2) {
+        r.SP = pad_mod16(r.R0, CC);
+        P = r.SP * r.R1;
+    } else {
+        r.SP = 1;
+        P = r.R0;
+    }
+    r.PP = pad_mod16(P, 1);
+    return r;
+}
+
+// coils per block: power of two covering the batch, at most 32 / NG, reduced
+// until the tile + staged samples fit in shared memory
+template <int NDIM, int W>
+static int cube_config(const Geom &g, int64_t batch, Region &rg, size_t &smem)
+{
+    using S = CubeShape<NDIM, W>;
+    const size_t limit = (size_t)max_smem();
+    int l = 0;
+    while ((1ll << l) < batch && (1 << l) * S::NG < 32) l++;
+    for (; l >= 0; l--) {
+        rg = cube_region<NDIM, W>(g, 1 << l);
+        smem = S::meta_bytes() + (size_t)(1 << l) * rg.PP * sizeof(float2);
+        if (smem <= limit) return l;
+    }
+    return -1;
+}
+
+template <int NDIM, int W>
+static int launch_interp_cube(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
+                              const float *weight, int wpb, cudaStream_t st)
+{
+    Region rg;
+    size_t smem = 0;
+    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem);
+    DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "interpolation tile does not fit in shared memory");
+    auto kern = interp_cube_kernel<NDIM, W>;
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t chunks = ceil_div(batch, 1ll << l);
+    DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+    kern<<<dim3(p->nwork, (unsigned)chunks), 256, smem, st>>>(p->g, rg, p->work, p->scoord[0], p->scoord[1],
+                                                            p->scoord[2], p->sidx, grid, ksp, batch,
+                                                            weight, wpb, (float)p->scale, l);
+    DMR_LAUNCHED("interp_cube_kernel");
+    return DMR_OK;
+}
+
+template <int NDIM, int W>
+static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                            const float *weight, int wpb, cudaStream_t st)
+{
+    Region rg;
+    size_t smem = 0;
+    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem);
+    DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "gridding tile does not fit in shared memory");
+    DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
+    if (p->nwork == 0) return DMR_OK;
+    auto kern = grid_cube_kernel<NDIM, W>;
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t chunks = ceil_div(batch, 1ll << l);
+    DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+    kern<<<dim3(p->nwork, (unsigned)chunks), 256, smem, st>>>(p->g, rg, p->work, p->scoord[0], p->scoord[1],
+                                                            p->scoord[2], p->sidx, ksp, kreal, grid, batch,
+                                                            weight, wpb, (float)p->scale, l);
+    DMR_LAUNCHED("grid_cube_kernel");
+    return DMR_OK;
+}
+
+// exact cube width instance for a plan: the widest axis, rounded up to an
+// instantiated width (1..8, 12, 16; 3D only up to 8); 0 = use the generic kernels
+static int cube_width(const Geom &g)
+{
+    int w = 1;
+    for (int a = 0; a < g.ndim; a++) w = std::max(w, g.W[a]);
+    if (w <= 8) return w;
+    if (g.ndim == 3) return 0;
+    return w <= 12 ? 12 : 16;
+}
+
+#define DMR_CUBE_CASES(F, ...)                                   \
+    case 101: return F<1, 1>(__VA_ARGS__);                       \
+    case 102: return F<1, 2>(__VA_ARGS__);                       \
+    case 103: return F<1, 3>(__VA_ARGS__);                       \
+    case 104: return F<1, 4>(__VA_ARGS__);                       \
+    case 105: return F<1, 5>(__VA_ARGS__);                       \
+    case 106: return F<1, 6>(__VA_ARGS__);                       \
+    case 107: return F<1, 7>(__VA_ARGS__);                       \
+    case 108: return F<1, 8>(__VA_ARGS__);                       \
+    case 112: return F<1, 12>(__VA_ARGS__);                      \
+    case 116: return F<1, 16>(__VA_ARGS__);                      \
+    case 201: return F<2, 1>(__VA_ARGS__);                       \
+    case 202: return F<2, 2>(__VA_ARGS__);                       \
+    case 203: return F<2, 3>(__VA_ARGS__);                       \
+    case 204: return F<2, 4>(__VA_ARGS__);                       \
+    case 205: return F<2, 5>(__VA_ARGS__);                       \
+    case 206: return F<2, 6>(__VA_ARGS__);                       \
+    case 207: return F<2, 7>(__VA_ARGS__);                       \
+    case 208: return F<2, 8>(__VA_ARGS__);                       \
+    case 212: return F<2, 12>(__VA_ARGS__);                      \
+    case 216: return F<2, 16>(__VA_ARGS__);                      \
+    case 301: return F<3, 1>(__VA_ARGS__);                       \
+    case 302: return F<3, 2>(__VA_ARGS__);                       \
+    case 303: return F<3, 3>(__VA_ARGS__);                       \
+    case 304: return F<3, 4>(__VA_ARGS__);                       \
+    case 305: return F<3, 5>(__VA_ARGS__);                       \
+    case 306: return F<3, 6>(__VA_ARGS__);                       \
+    case 307: return F<3, 7>(__VA_ARGS__);                       \
+    case 308: return F<3, 8>(__VA_ARGS__);
+
 int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
                     const float *weight, int wpb, cudaStream_t st)
 {
     if (p->nwork == 0) return DMR_OK;
+    const int cw = cube_width(p->g);
+    if (cw > 0) {
+        switch (p->g.ndim * 100 + cw) {
+            DMR_CUBE_CASES(launch_interp_cube, p, grid, ksp, batch, weight, wpb, st)
+        default: break;
+        }
+    }
     const int wm = wmax_for(p->g);
     switch (p->g.ndim * 100 + wm) {
     case 102: return launch_interp<1, 2>(p, grid, ksp, batch, weight, wpb, st);
@@ -642,6 +1068,13 @@ int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t 
 int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                   const float *weight, int wpb, int det, cudaStream_t st)
 {
+    const int cw = cube_width(p->g);
+    if (!det && cw > 0) {
+        switch (p->g.ndim * 100 + cw) {
+            DMR_CUBE_CASES(launch_grid_cube, p, ksp, kreal, grid, batch, weight, wpb, st)
+        default: break;
+        }
+    }
     const int wm = wmax_for(p->g);
     switch (p->g.ndim * 100 + wm) {
     case 102: return launch_grid<1, 2>(p, ksp, kreal, grid, batch, weight, wpb, det, st);
