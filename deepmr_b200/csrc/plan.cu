@@ -162,9 +162,11 @@ static double kernel_scale(const Geom &g)
 
 static void default_tile(int ndim, int T[3])
 {
-    if (ndim == 1) { T[0] = 1024; T[1] = T[2] = 1; }
-    else if (ndim == 2) { T[0] = 32; T[1] = 32; T[2] = 1; }
-    else { T[0] = 8; T[1] = 8; T[2] = 8; }
+    // bins = shared-memory tiles: a 32-coil tile + width-4 halo stays under
+    // ~100 KB (3D: 7^3 points, 2D: 19^2 points per coil)
+    if (ndim == 1) { T[0] = 256; T[1] = T[2] = 1; }
+    else if (ndim == 2) { T[0] = 16; T[1] = 16; T[2] = 1; }
+    else { T[0] = 4; T[1] = 4; T[2] = 4; }
 }
 
 template <typename T>
@@ -387,16 +389,15 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     std::vector<int32_t> h_start(nkeys + 1, 0);
     for (int64_t i = 0; i < nkeys; i++) h_start[i + 1] = h_start[i] + h_counts[i];
 
-    // interpolation / atomic-gridding items: non-empty bins in chunks, heavy first
-    const int kChunk = ndim == 3 ? 2048 : 4096;
+    // interpolation / atomic-gridding items: non-empty bins in chunks of at most
+    // kChunk samples (bounded work per block), in spatial order so that blocks
+    // running together share tile halos in L2
+    const int kChunk = 2048;
     std::vector<WorkItem> items;
     for (int64_t b = 0; b < nkeys; b++) {
         for (int s = h_start[b]; s < h_start[b + 1]; s += kChunk)
             items.push_back({(int)b, s, std::min(s + kChunk, h_start[b + 1])});
     }
-    std::stable_sort(items.begin(), items.end(), [](const WorkItem &x, const WorkItem &y) {
-        return (x.end - x.begin) > (y.end - y.begin);
-    });
 
     // owner-gridding tiles: every tile of every frame, ordered by the samples
     // of the bins that can reach it (the bin itself and its lower neighbours)

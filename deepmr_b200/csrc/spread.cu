@@ -344,18 +344,28 @@ __global__ void __launch_bounds__(256) grid_atomic_kernel(
 // in the kooshball / radial centre thousands of samples share a cell, so the
 // W^NDIM taps of a cell are held in registers and reused across the cell's
 // samples: interpolation reads the cube from the shared tile once per cell,
-// gridding accumulates into the cube and flushes it once per cell.
+// gridding accumulates into the cube and flushes it (shared atomics) once per
+// cell.
 //
-// Lane layout: lane = (stream s, slice g, coil c). A lane owns slice g of the
-// cube (one tap index along the outermost axis: z in 3D, y in 2D, x in 1D) for
-// coil c; NG = next power of two >= W slices, CC coils, NS = 32/(NG*CC)
-// independent sample streams per warp. Interpolation reduces the NG slice
-// partial sums with warp shuffles. Complex arithmetic uses the packed FP32
-// instructions (__ffma2_rn / __fmul2_rn).
+// Lane layout: lane = (stream s, slice group g, coil c). A lane owns SPL
+// consecutive slices of the cube (tap indices along the outermost axis: z in
+// 3D, y in 2D, x in 1D) for coil c: the whole cube (NG = 1) whenever it fits
+// in 64 complex registers, else NG groups of slices whose partial sums are
+// reduced with warp shuffles. CC coils and NS = 32/(NG*CC) independent sample
+// streams per warp. Complex arithmetic uses the packed FP32 instructions
+// (__ffma2_rn / __fmul2_rn).
 // ---------------------------------------------------------------------------
-template <int W>
-struct SliceGroups {
-    static constexpr int value = W <= 1 ? 1 : (W <= 2 ? 2 : (W <= 4 ? 4 : (W <= 8 ? 8 : 16)));
+template <int NDIM, int W>
+struct CubeShape {
+    static constexpr int INS = NDIM == 3 ? W * W : (NDIM == 2 ? W : 1);  // taps per slice
+    static constexpr int SPL0 = 64 / INS;                                 // slices that fit in 64 regs
+    static constexpr int SPL = SPL0 >= W ? W : (SPL0 < 1 ? 1 : SPL0);     // slices per lane
+    static constexpr int NGR = (W + SPL - 1) / SPL;                       // groups needed
+    static constexpr int NG = NGR <= 1 ? 1 : (NGR <= 2 ? 2 : (NGR <= 4 ? 4 : (NGR <= 8 ? 8 : 16)));
+    static constexpr int CUBE = SPL * INS;                                // complex registers
+    static constexpr int NW = NDIM * W;                                   // staged weights
+    static constexpr int SB = 256;                                        // staged samples
+    static size_t meta_bytes() { return (size_t)SB * (NW * sizeof(float) + 2 * sizeof(int)); }
 };
 
 // shared-memory geometry of the staged tile + halo for one coil chunk
@@ -365,15 +375,7 @@ struct Region {
     int PP;          // coil pitch (padded)
 };
 
-template <int NDIM, int W>
-struct CubeShape {
-    static constexpr int NG = SliceGroups<W>::value;
-    static constexpr int IN = NDIM == 3 ? W * W : (NDIM == 2 ? W : 1);  // taps per slice
-    static constexpr int NW = NDIM * W;                                  // staged weights
-    static constexpr int SB = NW <= 16 ? 256 : (NW <= 32 ? 128 : 64);    // staged samples
-    static size_t meta_bytes() { return (size_t)SB * (NW * sizeof(float) + 2 * sizeof(int)); }
-};
-
+// offset of tap j of a slice (row-major over the inner axes)
 template <int NDIM, int W>
 __device__ __forceinline__ int inner_off(int j, int R0)
 {
@@ -413,49 +415,78 @@ __device__ __forceinline__ void stage_cube_samples(const Geom &g, const int org[
     }
 }
 
-// stage (or, with `flush`, atomically add back) the tile + halo of CC coils
+// Stage (or, with `flush`, atomically add back scaled by inv_scale) the
+// tile + halo of CC coils, one grid row (R0 contiguous x) per thread step.
 template <int NDIM>
 __device__ __forceinline__ void region_io(const Geom &g, const Region &rg, const int org[3], int f,
                                           int64_t b0, int CC, int64_t batch, float2 *tile,
-                                          float2 *__restrict__ grid, bool flush, float scale)
+                                          float2 *__restrict__ grid, bool flush, float inv_scale)
 {
-    const int rows = rg.R1 * rg.R2;
-    const int per = rows * rg.R0;
-    for (int e = threadIdx.x; e < CC * per; e += blockDim.x) {
-        const int c = e / per;
-        const int r = e - c * per;
-        const int row = r / rg.R0;
-        const int rx = r - row * rg.R0;
-        const int ry = row % rg.R1;
-        const int rz = row / rg.R1;
-        const int si = c * rg.PP + (NDIM == 3 ? rz * rg.SP + ry * rg.R0 + rx : (NDIM == 2 ? ry * rg.SP + rx : rx));
+    const int rpc = rg.R1 * rg.R2;  // rows per coil
+    const int x_start = (org[0] + g.G[0] - g.half[0]) % g.G[0];
+    for (int row = threadIdx.x; row < CC * rpc; row += blockDim.x) {
+        const int c = row / rpc;
+        const int rr = row - c * rpc;
+        const int ry = rr % rg.R1;
+        const int rz = rr / rg.R1;
+        float2 *trow = tile + c * rg.PP + (NDIM == 3 ? rz * rg.SP + ry * rg.R0 : (NDIM == 2 ? ry * rg.SP : 0));
         const int64_t b = b0 + c;
         if (b >= batch) {
-            if (!flush) tile[si] = make_float2(0.0f, 0.0f);
+            if (!flush)
+                for (int rx = 0; rx < rg.R0; rx++) trow[rx] = make_float2(0.0f, 0.0f);
             continue;
         }
-        const int px = (org[0] + rx + g.G[0] - g.half[0]) % g.G[0];
         const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
         const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
-        float2 *gp = grid + (b * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0] + px;
+        float2 *grow = grid + (b * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0];
+        int px = x_start;
         if (!flush) {
-            tile[si] = *gp;
+            for (int rx = 0; rx < rg.R0; rx++) {
+                trow[rx] = grow[px];
+                px = (px + 1 == g.G[0]) ? 0 : px + 1;
+            }
         } else {
-            const float2 v = tile[si];
-            if (v.x != 0.0f || v.y != 0.0f) atomicAdd(gp, make_float2(v.x / scale, v.y / scale));
+            for (int rx = 0; rx < rg.R0; rx++) {
+                const float2 v = trow[rx];
+                if (v.x != 0.0f || v.y != 0.0f) atomicAdd(grow + px, __fmul2_rn(v, f2(inv_scale)));
+                px = (px + 1 == g.G[0]) ? 0 : px + 1;
+            }
         }
     }
 }
 
+struct LaneMap {
+    int c, gs, s, ns, stream, nstreams;
+    unsigned smask;
+};
+
+template <int NG>
+__device__ __forceinline__ LaneMap lane_map(int cc_log2)
+{
+    LaneMap m;
+    const int CC = 1 << cc_log2;
+    const int lane = threadIdx.x & 31;
+    m.c = lane & (CC - 1);
+    m.gs = (lane >> cc_log2) & (NG - 1);
+    m.s = lane / (CC * NG);
+    m.ns = 32 / (CC * NG);
+    m.stream = (threadIdx.x >> 5) * m.ns + m.s;
+    m.nstreams = (blockDim.x >> 5) * m.ns;
+    m.smask = (CC * NG == 32) ? 0xffffffffu : (((1u << (CC * NG)) - 1u) << (m.s * CC * NG));
+    return m;
+}
+
+constexpr int kCubeThreads = 128;
+
 template <int NDIM, int W>
-__global__ void __launch_bounds__(256) interp_cube_kernel(
+__global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
     const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
     const float2 *__restrict__ grid, float2 *__restrict__ ksp, int64_t batch,
-    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+    const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
 {
     using S = CubeShape<NDIM, W>;
-    constexpr int NG = S::NG, IN = S::IN, NW = S::NW;
+    constexpr int NG = S::NG, SPL = S::SPL, INS = S::INS, NW = S::NW;
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
     const WorkItem it = work[blockIdx.x];
@@ -469,95 +500,79 @@ __global__ void __launch_bounds__(256) interp_cube_kernel(
     const int64_t b0 = (int64_t)blockIdx.y * CC;
     region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, const_cast<float2 *>(grid), false, 1.0f);
 
-    const int lane = threadIdx.x & 31;
-    const int c = lane & (CC - 1);
-    const int gs = (lane >> cc_log2) & (NG - 1);
-    const int s = lane / (CC * NG);
-    const int ns = 32 / (CC * NG);
-    const int stream = (threadIdx.x >> 5) * ns + s;
-    const int nstreams = (blockDim.x >> 5) * ns;
-    const unsigned smask = (CC * NG == 32) ? 0xffffffffu : (((1u << (CC * NG)) - 1u) << (s * CC * NG));
-    const int64_t b = b0 + c;
+    const LaneMap m = lane_map<NG>(cc_log2);
+    const int64_t b = b0 + m.c;
+    const int z0 = m.gs * SPL;  // first slice of this lane
+    const float2 *ctile = tile + m.c * rg.PP + z0 * rg.SP;
 
     for (int base = it.begin; base < it.end; base += S::SB) {
         const int n = min(S::SB, it.end - base);
         __syncthreads();
         stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
         __syncthreads();
-        const int q0 = (int)((int64_t)n * stream / nstreams);
-        const int q1 = (int)((int64_t)n * (stream + 1) / nstreams);
+        const int q0 = (int)((int64_t)n * m.stream / m.nstreams);
+        const int q1 = (int)((int64_t)n * (m.stream + 1) / m.nstreams);
         int cur = -1;
-        float2 cube[IN];
-#pragma unroll
-        for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+        float2 cube[SPL][INS];
         for (int q = q0; q < q1; q++) {
             const int o = off[q];
             if (o != cur) {
                 cur = o;
-                if (gs < W) {
-                    const float2 *src = tile + c * rg.PP + o + gs * rg.SP;
 #pragma unroll
-                    for (int j = 0; j < IN; j++) cube[j] = src[inner_off<NDIM, W>(j, rg.R0)];
-                }
+                for (int sl = 0; sl < SPL; sl++)
+                    if (z0 + sl < W) {
+#pragma unroll
+                        for (int j = 0; j < INS; j++) cube[sl][j] = ctile[o + sl * rg.SP + inner_off<NDIM, W>(j, rg.R0)];
+                    }
             }
             const float *w = wts + q * NW;
             float2 acc = make_float2(0.0f, 0.0f);
-            if (NDIM == 3) {
 #pragma unroll
-                for (int jy = 0; jy < W; jy++) {
-                    float2 r = make_float2(0.0f, 0.0f);
+            for (int sl = 0; sl < SPL; sl++) {
+                if (z0 + sl >= W) continue;
+                float2 t = make_float2(0.0f, 0.0f);
+                if (NDIM == 3) {
 #pragma unroll
-                    for (int ix = 0; ix < W; ix++) r = __ffma2_rn(f2(w[ix]), cube[jy * W + ix], r);
-                    acc = __ffma2_rn(f2(w[W + jy]), r, acc);
+                    for (int jy = 0; jy < W; jy++) {
+                        float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+                        for (int ix = 0; ix < W; ix++) r = __ffma2_rn(f2(w[ix]), cube[sl][jy * W + ix], r);
+                        t = __ffma2_rn(f2(w[W + jy]), r, t);
+                    }
+                } else if (NDIM == 2) {
+#pragma unroll
+                    for (int ix = 0; ix < W; ix++) t = __ffma2_rn(f2(w[ix]), cube[sl][ix], t);
+                } else {
+                    t = cube[sl][0];
                 }
-            } else if (NDIM == 2) {
-#pragma unroll
-                for (int ix = 0; ix < W; ix++) acc = __ffma2_rn(f2(w[ix]), cube[ix], acc);
-            } else {
-                acc = cube[0];
+                acc = __ffma2_rn(f2(w[(NDIM - 1) * W + z0 + sl]), t, acc);
             }
-            const float wo = gs < W ? w[(NDIM - 1) * W + gs] : 0.0f;
-            acc = __fmul2_rn(f2(wo), acc);
+            if (NG > 1) {
 #pragma unroll
-            for (int m = 1; m < NG; m <<= 1) {
-                acc.x += __shfl_xor_sync(smask, acc.x, m * CC);
-                acc.y += __shfl_xor_sync(smask, acc.y, m * CC);
+                for (int k = 1; k < NG; k <<= 1) {
+                    acc.x += __shfl_xor_sync(m.smask, acc.x, k * CC);
+                    acc.y += __shfl_xor_sync(m.smask, acc.y, k * CC);
+                }
             }
-            if (gs == 0 && b < batch) {
+            if (m.gs == 0 && b < batch) {
                 const int64_t o2 = b * g.total + gi[q];
-                float2 y = make_float2(acc.x / scale, acc.y / scale);
-                if (weight) {
-                    const float wv = weight[wpb ? o2 : (int64_t)gi[q]];
-                    y.x *= wv;
-                    y.y *= wv;
-                }
-                ksp[o2] = y;
+                float sw = inv_scale;
+                if (weight) sw *= weight[wpb ? o2 : (int64_t)gi[q]];
+                ksp[o2] = __fmul2_rn(acc, f2(sw));
             }
         }
     }
 }
 
 template <int NDIM, int W>
-__device__ __forceinline__ void flush_cube(float2 *dst, const float2 *cube, int R0)
-{
-    constexpr int IN = CubeShape<NDIM, W>::IN;
-#pragma unroll
-    for (int j = 0; j < IN; j++) {
-        float2 *p = dst + inner_off<NDIM, W>(j, R0);
-        atomicAdd(&p->x, cube[j].x);
-        atomicAdd(&p->y, cube[j].y);
-    }
-}
-
-template <int NDIM, int W>
-__global__ void __launch_bounds__(256) grid_cube_kernel(
+__global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
     Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
     const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
     const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
-    const float *__restrict__ weight, int wpb, float scale, int cc_log2)
+    const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
 {
     using S = CubeShape<NDIM, W>;
-    constexpr int NG = S::NG, IN = S::IN, NW = S::NW;
+    constexpr int NG = S::NG, SPL = S::SPL, INS = S::INS, NW = S::NW;
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
     const WorkItem it = work[blockIdx.x];
@@ -571,64 +586,73 @@ __global__ void __launch_bounds__(256) grid_cube_kernel(
     for (int e = threadIdx.x; e < CC * rg.PP; e += blockDim.x) tile[e] = make_float2(0.0f, 0.0f);
     const int64_t b0 = (int64_t)blockIdx.y * CC;
 
-    const int lane = threadIdx.x & 31;
-    const int c = lane & (CC - 1);
-    const int gs = (lane >> cc_log2) & (NG - 1);
-    const int s = lane / (CC * NG);
-    const int ns = 32 / (CC * NG);
-    const int stream = (threadIdx.x >> 5) * ns + s;
-    const int nstreams = (blockDim.x >> 5) * ns;
-    const int64_t b = b0 + c;
-    const bool active = gs < W && b < batch;
+    const LaneMap m = lane_map<NG>(cc_log2);
+    const int64_t b = b0 + m.c;
+    const int z0 = m.gs * SPL;
+    const bool active = z0 < W && b < batch;
+    float2 *ctile = tile + m.c * rg.PP + z0 * rg.SP;
 
     for (int base = it.begin; base < it.end; base += S::SB) {
         const int n = min(S::SB, it.end - base);
         __syncthreads();
         stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
         __syncthreads();
-        const int q0 = (int)((int64_t)n * stream / nstreams);
-        const int q1 = (int)((int64_t)n * (stream + 1) / nstreams);
+        if (!active) continue;
+        const int q0 = (int)((int64_t)n * m.stream / m.nstreams);
+        const int q1 = (int)((int64_t)n * (m.stream + 1) / m.nstreams);
         int cur = -1;
-        float2 cube[IN];
+        float2 cube[SPL][INS];
 #pragma unroll
-        for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+        for (int sl = 0; sl < SPL; sl++)
+#pragma unroll
+            for (int j = 0; j < INS; j++) cube[sl][j] = make_float2(0.0f, 0.0f);
+        auto flush = [&](int o) {
+#pragma unroll
+            for (int sl = 0; sl < SPL; sl++)
+                if (z0 + sl < W) {
+#pragma unroll
+                    for (int j = 0; j < INS; j++) {
+                        float2 *p = ctile + o + sl * rg.SP + inner_off<NDIM, W>(j, rg.R0);
+                        atomicAdd(&p->x, cube[sl][j].x);
+                        atomicAdd(&p->y, cube[sl][j].y);
+                        cube[sl][j] = make_float2(0.0f, 0.0f);
+                    }
+                }
+        };
         for (int q = q0; q < q1; q++) {
             const int o = off[q];
             if (o != cur) {
-                if (cur >= 0 && active) flush_cube<NDIM, W>(tile + c * rg.PP + cur + gs * rg.SP, cube, rg.R0);
-#pragma unroll
-                for (int j = 0; j < IN; j++) cube[j] = make_float2(0.0f, 0.0f);
+                if (cur >= 0) flush(cur);
                 cur = o;
             }
-            if (!active) continue;
             const int64_t o2 = b * g.total + gi[q];
             float2 v = load_sample(ksp, kreal, o2);
-            if (weight) {
-                const float wv = weight[wpb ? o2 : (int64_t)gi[q]];
-                v.x *= wv;
-                v.y *= wv;
-            }
+            if (weight) v = __fmul2_rn(v, f2(weight[wpb ? o2 : (int64_t)gi[q]]));
             const float *w = wts + q * NW;
-            const float2 u = __fmul2_rn(f2(w[(NDIM - 1) * W + gs]), v);
-            if (NDIM == 3) {
 #pragma unroll
-                for (int jy = 0; jy < W; jy++) {
-                    const float2 t = __fmul2_rn(f2(w[W + jy]), u);
+            for (int sl = 0; sl < SPL; sl++) {
+                if (z0 + sl >= W) continue;
+                const float2 u = __fmul2_rn(f2(w[(NDIM - 1) * W + z0 + sl]), v);
+                if (NDIM == 3) {
 #pragma unroll
-                    for (int ix = 0; ix < W; ix++) cube[jy * W + ix] = __ffma2_rn(f2(w[ix]), t, cube[jy * W + ix]);
+                    for (int jy = 0; jy < W; jy++) {
+                        const float2 t = __fmul2_rn(f2(w[W + jy]), u);
+#pragma unroll
+                        for (int ix = 0; ix < W; ix++)
+                            cube[sl][jy * W + ix] = __ffma2_rn(f2(w[ix]), t, cube[sl][jy * W + ix]);
+                    }
+                } else if (NDIM == 2) {
+#pragma unroll
+                    for (int ix = 0; ix < W; ix++) cube[sl][ix] = __ffma2_rn(f2(w[ix]), u, cube[sl][ix]);
+                } else {
+                    cube[sl][0] = __fadd2_rn(cube[sl][0], u);
                 }
-            } else if (NDIM == 2) {
-#pragma unroll
-                for (int ix = 0; ix < W; ix++) cube[ix] = __ffma2_rn(f2(w[ix]), u, cube[ix]);
-            } else {
-                cube[0].x += u.x;
-                cube[0].y += u.y;
             }
         }
-        if (cur >= 0 && active) flush_cube<NDIM, W>(tile + c * rg.PP + cur + gs * rg.SP, cube, rg.R0);
+        if (cur >= 0) flush(cur);
     }
     __syncthreads();
-    region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, scale);
+    region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -917,16 +941,22 @@ static int pad_mod16(int x, int m)
 template <int NDIM, int W>
 static Region cube_region(const Geom &g, int CC)
 {
+    using S = CubeShape<NDIM, W>;
     Region r;
     r.R0 = g.T[0] + W - 1;
     r.R1 = NDIM > 1 ? g.T[1] + W - 1 : 1;
     r.R2 = NDIM > 2 ? g.T[2] + W - 1 : 1;
+    // lanes of one half-warp differ in coil (pitch PP = 1 mod 16) and, with NG > 1,
+    // in slice group (pitch SPL * SP = CC mod 16), so 8-byte accesses spread over banks
+    const int want = (S::NG > 1) ? CC : 0;
     int P;
     if (NDIM == 3) {
-        r.SP = pad_mod16(r.R0 * r.R1, CC);
+        r.SP = r.R0 * r.R1;
+        while (S::NG > 1 && ((S::SPL * r.SP) & 15) != (want & 15)) r.SP++;
         P = r.SP * r.R2;
     } else if (NDIM == 2) {
-        r.SP = pad_mod16(r.R0, CC);
+        r.SP = r.R0;
+        while (S::NG > 1 && ((S::SPL * r.SP) & 15) != (want & 15)) r.SP++;
         P = r.SP * r.R1;
     } else {
         r.SP = 1;
@@ -965,9 +995,9 @@ static int launch_interp_cube(const dmr_plan *p, const float2 *grid, float2 *ksp
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t chunks = ceil_div(batch, 1ll << l);
     DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
-    kern<<<dim3(p->nwork, (unsigned)chunks), 256, smem, st>>>(p->g, rg, p->work, p->scoord[0], p->scoord[1],
-                                                            p->scoord[2], p->sidx, grid, ksp, batch,
-                                                            weight, wpb, (float)p->scale, l);
+    kern<<<dim3(p->nwork, (unsigned)chunks), kCubeThreads, smem, st>>>(
+        p->g, rg, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx, grid, ksp, batch, weight,
+        wpb, (float)(1.0 / p->scale), l);
     DMR_LAUNCHED("interp_cube_kernel");
     return DMR_OK;
 }
@@ -986,9 +1016,9 @@ static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t chunks = ceil_div(batch, 1ll << l);
     DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
-    kern<<<dim3(p->nwork, (unsigned)chunks), 256, smem, st>>>(p->g, rg, p->work, p->scoord[0], p->scoord[1],
-                                                            p->scoord[2], p->sidx, ksp, kreal, grid, batch,
-                                                            weight, wpb, (float)p->scale, l);
+    kern<<<dim3(p->nwork, (unsigned)chunks), kCubeThreads, smem, st>>>(
+        p->g, rg, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid, batch,
+        weight, wpb, (float)(1.0 / p->scale), l);
     DMR_LAUNCHED("grid_cube_kernel");
     return DMR_OK;
 }
