@@ -948,15 +948,20 @@ static Region cube_region(const Geom &g, int CC)
     r.R2 = NDIM > 2 ? g.T[2] + W - 1 : 1;
     // lanes of one half-warp differ in coil (pitch PP = 1 mod 16) and, with NG > 1,
     // in slice group (pitch SPL * SP = CC mod 16), so 8-byte accesses spread over banks
-    const int want = (S::NG > 1) ? CC : 0;
+    // (the congruence may have no solution, e.g. SPL even and CC odd: then keep
+    // the unpadded pitch; the search is bounded to one period)
+    auto pad_slice = [&](int sp) {
+        if (S::NG == 1) return sp;
+        for (int d = 0; d < 16; d++)
+            if (((S::SPL * (sp + d)) & 15) == (CC & 15)) return sp + d;
+        return sp;
+    };
     int P;
     if (NDIM == 3) {
-        r.SP = r.R0 * r.R1;
-        while (S::NG > 1 && ((S::SPL * r.SP) & 15) != (want & 15)) r.SP++;
+        r.SP = pad_slice(r.R0 * r.R1);
         P = r.SP * r.R2;
     } else if (NDIM == 2) {
-        r.SP = r.R0;
-        while (S::NG > 1 && ((S::SPL * r.SP) & 15) != (want & 15)) r.SP++;
+        r.SP = pad_slice(r.R0);
         P = r.SP * r.R1;
     } else {
         r.SP = 1;
