@@ -455,6 +455,48 @@ __device__ __forceinline__ void region_io(const Geom &g, const Region &rg, const
     }
 }
 
+// Asynchronous 8-byte global -> shared copies (cp.async), so a block can stage
+// its tile + halo while it computes sample weights.
+__device__ __forceinline__ void cp_async8(void *sdst, const void *gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int NDIM>
+__device__ __forceinline__ void region_load_async(const Geom &g, const Region &rg, const int org[3], int f,
+                                                  int64_t b0, int CC, int64_t batch, float2 *tile,
+                                                  const float2 *__restrict__ grid)
+{
+    const int rpc = rg.R1 * rg.R2;
+    const int x_start = (org[0] + g.G[0] - g.half[0]) % g.G[0];
+    for (int row = threadIdx.x; row < CC * rpc; row += blockDim.x) {
+        const int c = row / rpc;
+        const int rr = row - c * rpc;
+        const int ry = rr % rg.R1;
+        const int rz = rr / rg.R1;
+        float2 *trow = tile + c * rg.PP + (NDIM == 3 ? rz * rg.SP + ry * rg.R0 : (NDIM == 2 ? ry * rg.SP : 0));
+        const int64_t b = b0 + c;
+        if (b >= batch) {
+            for (int rx = 0; rx < rg.R0; rx++) trow[rx] = make_float2(0.0f, 0.0f);
+            continue;
+        }
+        const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+        const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+        const float2 *grow = grid + (b * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0];
+        int px = x_start;
+        for (int rx = 0; rx < rg.R0; rx++) {
+            cp_async8(trow + rx, grow + px);
+            px = (px + 1 == g.G[0]) ? 0 : px + 1;
+        }
+    }
+}
+
 struct LaneMap {
     int c, gs, s, ns, stream, nstreams;
     unsigned smask;
@@ -498,7 +540,8 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     int *off = reinterpret_cast<int *>(wts + S::SB * NW);
     int *gi = off + S::SB;
     const int64_t b0 = (int64_t)blockIdx.y * CC;
-    region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, const_cast<float2 *>(grid), false, 1.0f);
+    // tile copies in flight while the first batch of weights is computed
+    region_load_async<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid);
 
     const LaneMap m = lane_map<NG>(cc_log2);
     const int64_t b = b0 + m.c;
@@ -507,8 +550,9 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
 
     for (int base = it.begin; base < it.end; base += S::SB) {
         const int n = min(S::SB, it.end - base);
-        __syncthreads();
+        if (base != it.begin) __syncthreads();
         stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
+        if (base == it.begin) cp_async_wait_all();
         __syncthreads();
         const int q0 = (int)((int64_t)n * m.stream / m.nstreams);
         const int q1 = (int)((int64_t)n * (m.stream + 1) / m.nstreams);
@@ -653,6 +697,103 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
     }
     __syncthreads();
     region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
+}
+
+// ---------------------------------------------------------------------------
+// 3D gridding by z-slab ownership. Block = W warps; warp w owns the tile planes
+// congruent to w modulo W, so of every sample's W x W x W taps it handles the
+// one z plane that falls in its planes. All warps walk all samples of the bin
+// in sorted (cell) order; lane (row group rr, coil c) owns rows dy = rr (mod
+// NR) of that plane for coil c and accumulates them in registers while the
+// cell does not change, then adds them to the shared tile with plain
+// read-modify-writes: every (point, coil) has exactly one owner lane, so there
+// are no shared-memory atomics and each tile sums in a fixed order. The tile +
+// halo is finally added to the grid with global vector atomics.
+// ---------------------------------------------------------------------------
+template <int W, int NR>
+__global__ void __launch_bounds__(32 * W) grid_slab_kernel(
+    Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
+    const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
+    const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
+    const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
+{
+    using S = CubeShape<3, W>;
+    constexpr int NW = S::NW;
+    constexpr int RL = (W + NR - 1) / NR;  // rows per lane
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int CC = 1 << cc_log2;
+    const WorkItem it = work[blockIdx.x];
+    const int f = it.bin / g.nbins;
+    int org[3];
+    tile_origin(g, it.bin - f * g.nbins, org);
+    float2 *tile = reinterpret_cast<float2 *>(smem);
+    float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
+    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *gi = off + S::SB;
+    for (int e = threadIdx.x; e < CC * rg.PP; e += blockDim.x) tile[e] = make_float2(0.0f, 0.0f);
+    const int64_t b0 = (int64_t)blockIdx.y * CC;
+
+    const int lane = threadIdx.x & 31;
+    const int wz = threadIdx.x >> 5;  // owned planes: wz (mod W)
+    const int c = lane & (CC - 1);
+    const int rr = lane >> cc_log2;  // row group
+    const int64_t b = b0 + c;
+    const bool active = b < batch && rr < NR && rr < W;
+    float2 *ctile = tile + c * rg.PP;
+
+    for (int base = it.begin; base < it.end; base += S::SB) {
+        const int n = min(S::SB, it.end - base);
+        __syncthreads();
+        stage_cube_samples<3, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
+        __syncthreads();
+        if (!active) continue;
+        int cur = -1, dz = 0;
+        float2 acc[RL][W];
+#pragma unroll
+        for (int k = 0; k < RL; k++)
+#pragma unroll
+            for (int i = 0; i < W; i++) acc[k][i] = make_float2(0.0f, 0.0f);
+        auto flush = [&](int o) {
+            float2 *pl = ctile + o + dz * rg.SP;
+#pragma unroll
+            for (int k = 0; k < RL; k++) {
+                const int dy = rr + NR * k;
+                if (dy >= W) continue;
+                float2 *row = pl + dy * rg.R0;
+#pragma unroll
+                for (int i = 0; i < W; i++) {
+                    row[i] = __fadd2_rn(row[i], acc[k][i]);
+                    acc[k][i] = make_float2(0.0f, 0.0f);
+                }
+            }
+        };
+        for (int q = 0; q < n; q++) {
+            const int o = off[q];
+            if (o != cur) {
+                if (cur >= 0) flush(cur);
+                cur = o;
+                const int lz = o / rg.SP;  // plane of the first tap
+                dz = wz - lz % W;
+                if (dz < 0) dz += W;
+            }
+            const int64_t o2 = b * g.total + gi[q];
+            float2 v = load_sample(ksp, kreal, o2);
+            if (weight) v = __fmul2_rn(v, f2(weight[wpb ? o2 : (int64_t)gi[q]]));
+            const float *w = wts + q * NW;
+            const float2 u = __fmul2_rn(f2(w[2 * W + dz]), v);
+#pragma unroll
+            for (int k = 0; k < RL; k++) {
+                const int dy = rr + NR * k;
+                if (dy >= W) continue;
+                const float2 t = __fmul2_rn(f2(w[W + dy]), u);
+#pragma unroll
+                for (int i = 0; i < W; i++) acc[k][i] = __ffma2_rn(f2(w[i]), t, acc[k][i]);
+            }
+        }
+        if (cur >= 0) flush(cur);
+    }
+    __syncthreads();
+    region_io<3>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -1028,6 +1169,52 @@ static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float
     return DMR_OK;
 }
 
+// 3D gridding with the slab kernel: CC = min(32, pow2 >= batch) coils, NR = 32 / CC
+// row groups (capped at W; extra lanes idle)
+template <int W, int NR>
+static int launch_grid_slab_nr(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                               const float *weight, int wpb, int l, const Region &rg, size_t smem,
+                               cudaStream_t st)
+{
+    auto kern = grid_slab_kernel<W, NR>;
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t chunks = ceil_div(batch, 1ll << l);
+    DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
+    kern<<<dim3(p->nwork, (unsigned)chunks), 32 * W, smem, st>>>(
+        p->g, rg, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid, batch,
+        weight, wpb, (float)(1.0 / p->scale), l);
+    DMR_LAUNCHED("grid_slab_kernel");
+    return DMR_OK;
+}
+
+template <int NDIM, int W>
+static int launch_grid_slab(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                            const float *weight, int wpb, cudaStream_t st)
+{
+    using S = CubeShape<3, W>;
+    const size_t limit = (size_t)max_smem();
+    int l = 0;
+    while ((1ll << l) < batch && l < 5) l++;
+    Region rg;
+    size_t smem = 0;
+    for (; l >= 0; l--) {
+        rg = cube_region<3, W>(p->g, 1 << l);
+        smem = S::meta_bytes() + (size_t)(1 << l) * rg.PP * sizeof(float2);
+        if (smem <= limit) break;
+    }
+    DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "gridding tile does not fit in shared memory");
+    DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
+    if (p->nwork == 0) return DMR_OK;
+    switch (l) {
+    case 5: return launch_grid_slab_nr<W, 1>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 4: return launch_grid_slab_nr<W, 2>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 3: return launch_grid_slab_nr<W, 4>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 2: return launch_grid_slab_nr<W, 8>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 1: return launch_grid_slab_nr<W, 16>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    default: return launch_grid_slab_nr<W, 32>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    }
+}
+
 // exact cube width instance for a plan: the widest axis, rounded up to an
 // instantiated width (1..8, 12, 16; 3D only up to 8); 0 = use the generic kernels
 static int cube_width(const Geom &g)
@@ -1104,6 +1291,19 @@ int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, i
                   const float *weight, int wpb, int det, cudaStream_t st)
 {
     const int cw = cube_width(p->g);
+    if (!det && cw > 0 && p->g.ndim == 3) {
+        switch (cw) {
+        case 1: return launch_grid_slab<3, 1>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 2: return launch_grid_slab<3, 2>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 3: return launch_grid_slab<3, 3>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 4: return launch_grid_slab<3, 4>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 5: return launch_grid_slab<3, 5>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 6: return launch_grid_slab<3, 6>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 7: return launch_grid_slab<3, 7>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        case 8: return launch_grid_slab<3, 8>(p, ksp, kreal, grid, batch, weight, wpb, st);
+        default: break;
+        }
+    }
     if (!det && cw > 0) {
         switch (p->g.ndim * 100 + cw) {
             DMR_CUBE_CASES(launch_grid_cube, p, ksp, kreal, grid, batch, weight, wpb, st)
