@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--small", action="store_true", help="reduced workload (profiling)")
+    ap.add_argument("--medium", action="store_true", help="32-coil 128^3 workload (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip Toeplitz / per-kernel timing")
@@ -55,6 +56,8 @@ def workload(args):
     w = dict(WORKLOAD)
     if args.small:
         w.update(N=128, coils=8, spokes=25000, samples=256)
+    if getattr(args, "medium", False):
+        w.update(N=128, coils=32, spokes=25000, samples=256)
     return w
 
 
@@ -324,6 +327,9 @@ def run_b200(args):
             x = F.apply_nufft_adj(ksp_h, plan, weight=dcf)
             return y, x
 
+        # two untimed calls so the pinned-host caching allocator holds both
+        # generations of output buffers (a fresh pinned allocation is not a copy)
+        y_h, x_h = estep()
         y_h, x_h = estep()
         torch.cuda.synchronize()
         barrier(world)

@@ -15,6 +15,7 @@
 // centred index c of an axis is stored at (c - G//2) mod G — so the fftshift
 // of the reference's centred FFT (src/deepmr/fft/fft.py:77-80) costs nothing.
 #include <algorithm>
+#include <cstdlib>
 
 #include "kb.cuh"
 #include "plan.cuh"
@@ -1215,6 +1216,17 @@ static int launch_grid_slab(const dmr_plan *p, const void *ksp, int kreal, float
     }
 }
 
+// 3D gridding kernel choice: 0 = cell-cube kernel (shared atomics per cell),
+// 1 = z-slab kernel; DMR_GRID_VARIANT overrides the default (tuning only)
+static int grid_variant()
+{
+    static int v = [] {
+        const char *e = getenv("DMR_GRID_VARIANT");
+        return e ? atoi(e) : 0;
+    }();
+    return v;
+}
+
 // exact cube width instance for a plan: the widest axis, rounded up to an
 // instantiated width (1..8, 12, 16; 3D only up to 8); 0 = use the generic kernels
 static int cube_width(const Geom &g)
@@ -1291,7 +1303,7 @@ int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, i
                   const float *weight, int wpb, int det, cudaStream_t st)
 {
     const int cw = cube_width(p->g);
-    if (!det && cw > 0 && p->g.ndim == 3) {
+    if (!det && cw > 0 && p->g.ndim == 3 && grid_variant() == 1) {
         switch (cw) {
         case 1: return launch_grid_slab<3, 1>(p, ksp, kreal, grid, batch, weight, wpb, st);
         case 2: return launch_grid_slab<3, 2>(p, ksp, kreal, grid, batch, weight, wpb, st);
