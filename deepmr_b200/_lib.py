@@ -42,6 +42,7 @@ SYMBOLS = (
     "dmr_toeplitz_workspace_bytes",
     "dmr_toeplitz_finalize",
     "dmr_toeplitz_apply",
+    "dmr_toeplitz_normalize_noalloc",
 )
 
 
@@ -96,6 +97,7 @@ _SIGS = {
         ctypes.c_int,
         [ctypes.c_int, i32p, i32p, vp, i64, vp, ctypes.c_int, vp, i64, vp, ctypes.c_size_t, vp],
     ),
+    "dmr_toeplitz_normalize_noalloc": (ctypes.c_int, [vp, i64, vp]),
 }
 
 

@@ -506,3 +506,94 @@ extern "C" int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t
     c.isize = ksize;
     return launch_resize(c, data, (float2 *)out, st);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free Toeplitz kernel normalisation (dmr_toeplitz_normalize_noalloc).
+//
+// For callers that may not allocate device memory: the partial sums of the
+// |k| reduction live in a file-scope static device array instead of a caller
+// workspace. The array is a fixed 64 KB that every device loading this
+// library keeps until process exit; it holds kNoAllocParts partial results of
+// kNoAllocPerPart elements each, which bounds the input size.
+// ---------------------------------------------------------------------------
+namespace dmr {
+
+constexpr int kNoAllocParts = 4096;
+constexpr int64_t kNoAllocPerPart = 16384;
+constexpr int64_t kNoAllocMaxElems = (int64_t)kNoAllocParts * kNoAllocPerPart;  // 67,108,864
+
+// partial sums in [0, kNoAllocParts), partial counts (as 64-bit integers) after
+static __device__ __align__(256) double g_norm_scratch[2 * kNoAllocParts];
+
+// one contiguous slice of kNoAllocPerPart elements per block
+__global__ void absmean_slice_kernel(const float2 *__restrict__ k, int64_t n, int64_t per_part,
+                                     double *__restrict__ sums, unsigned long long *__restrict__ counts)
+{
+    const int64_t lo = blockIdx.x * per_part;
+    const int64_t hi = min(n, lo + per_part);
+    double s = 0.0;
+    unsigned long long c = 0;
+    for (int64_t e = lo + threadIdx.x; e < hi; e += blockDim.x) {
+        const float2 v = k[e];
+        if (v.x != 0.0f || v.y != 0.0f) {
+            s += (double)hypotf(v.x, v.y);
+            c++;
+        }
+    }
+    __shared__ double ss[256];
+    __shared__ unsigned long long sc[256];
+    ss[threadIdx.x] = s;
+    sc[threadIdx.x] = c;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            ss[threadIdx.x] += ss[threadIdx.x + h];
+            sc[threadIdx.x] += sc[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {  // every partial is overwritten: nothing needs clearing
+        sums[blockIdx.x] = ss[0];
+        counts[blockIdx.x] = sc[0];
+    }
+}
+
+// Device address of g_norm_scratch for the current device, looked up once per
+// device with that device current (the host-side name is only a stand-in).
+static int norm_scratch(double **out)
+{
+    static std::mutex mu;
+    static double *addr[128] = {};
+    int dev = 0;
+    DMR_CUDA(cudaGetDevice(&dev));
+    DMR_CHECK(dev >= 0 && dev < 128, DMR_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        DMR_CUDA(cudaGetSymbolAddress(&p, g_norm_scratch));
+        addr[dev] = (double *)p;
+    }
+    *out = addr[dev];
+    return DMR_OK;
+}
+
+}  // namespace dmr
+
+extern "C" int dmr_toeplitz_normalize_noalloc(void *kernel, int64_t n, void *stream)
+{
+    DMR_CHECK(kernel && n >= 1, DMR_ERR_INVALID, "bad argument");
+    DMR_CHECK(n <= kNoAllocMaxElems, DMR_ERR_INVALID,
+              "n = %lld exceeds the %lld-element maximum of the allocation-free normalisation "
+              "(use dmr_toeplitz_finalize with a workspace)",
+              (long long)n, (long long)kNoAllocMaxElems);
+    cudaStream_t st = (cudaStream_t)stream;
+    double *sums = nullptr;
+    DMR_TRY(norm_scratch(&sums));
+    unsigned long long *counts = reinterpret_cast<unsigned long long *>(sums + kNoAllocParts);
+    const int nparts = (int)ceil_div(n, kNoAllocPerPart);
+    absmean_slice_kernel<<<nparts, 256, 0, st>>>((const float2 *)kernel, n, kNoAllocPerPart, sums, counts);
+    DMR_LAUNCHED("absmean_slice_kernel");
+    normalise_kernel<<<elem_blocks(n), 256, 0, st>>>((float2 *)kernel, n, sums, counts, nparts);
+    DMR_LAUNCHED("normalise_kernel");
+    return DMR_OK;
+}

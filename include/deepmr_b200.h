@@ -189,6 +189,27 @@ int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t *ishape,
                        int image_real, void *out, int64_t batch,
                        void *workspace, size_t workspace_bytes, void *stream);
 
+/*
+ * Allocation-free variant of the Toeplitz kernel normalisation step.
+ * No counterpart in the reference. For callers that must not allocate device
+ * memory (an application that hands the GPU a fixed memory pool at start-up,
+ * a real-time reconstruction loop that forbids allocator calls once running,
+ * or a host without a CUDA allocator of its own): scales the complex64 array
+ * `kernel` (n elements) in place by 1 / mean(|k| over k != 0) and replaces
+ * NaN by 0 and +-inf by +-FLT_MAX — the normalisation of dmr_toeplitz_finalize
+ * — with the reduction's partial sums in a 64 KB static device array owned by
+ * the library (kept by every device that loads it until the process exits)
+ * instead of a caller workspace. Calls no allocator.
+ *  - n must not exceed 67,108,864 elements (4096 partial sums x 16384
+ *    elements); larger n returns DMR_ERR_INVALID.
+ *  - The first call on a device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU (different
+ *    streams, or different host threads) race and give wrong results.
+ */
+int dmr_toeplitz_normalize_noalloc(void *kernel, int64_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
