@@ -431,6 +431,55 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     std::vector<int32_t> order(tc.size());
     for (size_t i = 0; i < tc.size(); i++) order[i] = tc[i].second;
 
+    // deterministic gridding: colour bins so that same-colour tile + halo
+    // regions [b*T, b*T + T + Wmax - 1) (mod G) are disjoint on some axis;
+    // along each axis colour = b mod C with the smallest conflict-free C
+    int wmax = 1;
+    for (int a = 0; a < ndim; a++) wmax = std::max(wmax, g.W[a]);
+    int C[3] = {1, 1, 1};
+    for (int a = 0; a < 3; a++) {
+        const int nb = g.nb[a];
+        const int ext = g.T[a] + (a < ndim ? wmax : 1) - 1;
+        for (C[a] = std::max(1, (int)ceil_div(ext, g.T[a])); C[a] < nb; C[a]++) {
+            bool ok = true;
+            for (int b1 = 0; b1 < nb && ok; b1++)
+                for (int b2 = b1 + 1; b2 < nb && ok; b2++) {
+                    if (b1 % C[a] != b2 % C[a]) continue;
+                    // regions as sets of grid indices mod G
+                    for (int i = 0; i < ext && ok; i++) {
+                        const int x = (b1 * g.T[a] + i) % g.G[a];
+                        const int d = pmod(x - b2 * g.T[a], g.G[a]);
+                        if (d < ext) ok = false;
+                    }
+                }
+            if (ok) break;
+        }
+        C[a] = std::min(C[a], nb);
+    }
+    const int ncolors = C[0] * C[1] * C[2];
+    std::vector<std::vector<WorkItem>> by_color(ncolors);
+    for (int64_t key = 0; key < nkeys; key++) {
+        if (h_start[key + 1] == h_start[key]) continue;
+        const int lb = (int)(key % g.nbins);
+        const int bx = lb % g.nb[0], by = (lb / g.nb[0]) % g.nb[1], bz = lb / (g.nb[0] * g.nb[1]);
+        const int col = (bz % C[2] * C[1] + by % C[1]) * C[0] + bx % C[0];
+        by_color[col].push_back({(int)key, h_start[key], h_start[key + 1]});
+    }
+    std::vector<WorkItem> det;
+    p->det_color_start.assign(1, 0);
+    for (int c = 0; c < ncolors; c++) {
+        // heaviest bins first inside a pass (shorter tail)
+        std::stable_sort(by_color[c].begin(), by_color[c].end(), [](const WorkItem &x, const WorkItem &y) {
+            return (x.end - x.begin) > (y.end - y.begin);
+        });
+        det.insert(det.end(), by_color[c].begin(), by_color[c].end());
+        p->det_color_start.push_back((int)det.size());
+    }
+    DMR_TRY(dev_alloc(&p->det_work, det.size()));
+    if (!det.empty())
+        DMR_CUDA(cudaMemcpyAsync(p->det_work, det.data(), det.size() * sizeof(WorkItem),
+                                 cudaMemcpyHostToDevice, st));
+
     p->nwork = (int)items.size();
     p->ntiles = (int)order.size();
     DMR_TRY(dev_alloc(&p->bin_start, nkeys + 1));

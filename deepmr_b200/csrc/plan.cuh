@@ -64,6 +64,10 @@ struct dmr_plan {
     int nwork = 0;
     int32_t *tiles = nullptr;           // owner-gridding tile order (heavy first)
     int ntiles = 0;
+    // deterministic gridding: whole non-empty bins grouped by colour; bins of
+    // one colour have disjoint tile + halo regions
+    dmr::WorkItem *det_work = nullptr;
+    std::vector<int> det_color_start;   // host, ncolors + 1
     float *apod[3] = {nullptr, nullptr, nullptr};  // per-axis apodisation (image index)
 
     ~dmr_plan()
@@ -76,5 +80,6 @@ struct dmr_plan {
         cudaFree(bin_start);
         cudaFree(work);
         cudaFree(tiles);
+        cudaFree(det_work);
     }
 };

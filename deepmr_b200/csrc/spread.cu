@@ -701,26 +701,30 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
 }
 
 // ---------------------------------------------------------------------------
-// 3D gridding by z-slab ownership. Block = W warps; warp w owns the tile planes
-// congruent to w modulo W, so of every sample's W x W x W taps it handles the
-// one z plane that falls in its planes. All warps walk all samples of the bin
-// in sorted (cell) order; lane (row group rr, coil c) owns rows dy = rr (mod
-// NR) of that plane for coil c and accumulates them in registers while the
-// cell does not change, then adds them to the shared tile with plain
-// read-modify-writes: every (point, coil) has exactly one owner lane, so there
-// are no shared-memory atomics and each tile sums in a fixed order. The tile +
-// halo is finally added to the grid with global vector atomics.
+// Gridding by slab ownership. Block = W warps; warp w owns the tile slices
+// (outermost axis: z in 3D, y in 2D, x in 1D) congruent to w modulo W, so of
+// every sample's W^NDIM taps it handles the one slice that falls in its own.
+// All warps walk all samples of the bin in sorted (cell) order; lane (group
+// rr, coil c) owns the taps of that slice whose next-axis offset (y in 3D, x
+// in 2D) is congruent to rr modulo NR, for coil c, and accumulates them in
+// registers while the cell does not change, then adds them to the shared tile
+// with plain read-modify-writes. Every (point, coil) has exactly one owner
+// lane, so there are no shared-memory atomics and each tile sums in a fixed
+// order. The tile + halo is then added to the grid: with global atomics, or
+// (deterministic mode) with plain read-modify-writes, the launcher running
+// the bins in colour passes whose tile + halo regions are disjoint.
 // ---------------------------------------------------------------------------
-template <int W, int NR>
+template <int NDIM, int W, int NR, bool ATOMIC_FLUSH>
 __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
     Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
     const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
     const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
     const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
 {
-    using S = CubeShape<3, W>;
+    using S = CubeShape<NDIM, W>;
     constexpr int NW = S::NW;
-    constexpr int RL = (W + NR - 1) / NR;  // rows per lane
+    constexpr int RL = NDIM == 1 ? 1 : (W + NR - 1) / NR;  // owned next-axis taps per lane
+    constexpr int CL = NDIM == 3 ? W : 1;                  // x taps per owned row (3D)
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
     const WorkItem it = work[blockIdx.x];
@@ -735,34 +739,35 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
     const int64_t b0 = (int64_t)blockIdx.y * CC;
 
     const int lane = threadIdx.x & 31;
-    const int wz = threadIdx.x >> 5;  // owned planes: wz (mod W)
+    const int wz = threadIdx.x >> 5;  // owned slices: wz (mod W)
     const int c = lane & (CC - 1);
-    const int rr = lane >> cc_log2;  // row group
+    const int rr = lane >> cc_log2;  // tap group on the next axis
     const int64_t b = b0 + c;
-    const bool active = b < batch && rr < NR && rr < W;
+    const bool active = b < batch && (NDIM == 1 ? rr == 0 : (rr < NR && rr < W));
     float2 *ctile = tile + c * rg.PP;
+    const int nstride = NDIM == 3 ? rg.R0 : 1;  // pitch of the next axis
 
     for (int base = it.begin; base < it.end; base += S::SB) {
         const int n = min(S::SB, it.end - base);
         __syncthreads();
-        stage_cube_samples<3, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
+        stage_cube_samples<NDIM, W>(g, org, rg, base, n, sc0, sc1, sc2, sidx, wts, off, gi);
         __syncthreads();
         if (!active) continue;
         int cur = -1, dz = 0;
-        float2 acc[RL][W];
+        float2 acc[RL][CL];
 #pragma unroll
         for (int k = 0; k < RL; k++)
 #pragma unroll
-            for (int i = 0; i < W; i++) acc[k][i] = make_float2(0.0f, 0.0f);
+            for (int i = 0; i < CL; i++) acc[k][i] = make_float2(0.0f, 0.0f);
         auto flush = [&](int o) {
             float2 *pl = ctile + o + dz * rg.SP;
 #pragma unroll
             for (int k = 0; k < RL; k++) {
                 const int dy = rr + NR * k;
-                if (dy >= W) continue;
-                float2 *row = pl + dy * rg.R0;
+                if (NDIM > 1 && dy >= W) continue;
+                float2 *row = pl + (NDIM == 1 ? 0 : dy * nstride);
 #pragma unroll
-                for (int i = 0; i < W; i++) {
+                for (int i = 0; i < CL; i++) {
                     row[i] = __fadd2_rn(row[i], acc[k][i]);
                     acc[k][i] = make_float2(0.0f, 0.0f);
                 }
@@ -773,7 +778,7 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
             if (o != cur) {
                 if (cur >= 0) flush(cur);
                 cur = o;
-                const int lz = o / rg.SP;  // plane of the first tap
+                const int lz = o / rg.SP;  // outermost index of the first tap
                 dz = wz - lz % W;
                 if (dz < 0) dz += W;
             }
@@ -781,20 +786,50 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
             float2 v = load_sample(ksp, kreal, o2);
             if (weight) v = __fmul2_rn(v, f2(weight[wpb ? o2 : (int64_t)gi[q]]));
             const float *w = wts + q * NW;
-            const float2 u = __fmul2_rn(f2(w[2 * W + dz]), v);
+            const float2 u = __fmul2_rn(f2(w[(NDIM - 1) * W + dz]), v);
 #pragma unroll
             for (int k = 0; k < RL; k++) {
                 const int dy = rr + NR * k;
-                if (dy >= W) continue;
-                const float2 t = __fmul2_rn(f2(w[W + dy]), u);
+                if (NDIM > 1 && dy >= W) continue;
+                if (NDIM == 3) {
+                    const float2 t = __fmul2_rn(f2(w[W + dy]), u);
 #pragma unroll
-                for (int i = 0; i < W; i++) acc[k][i] = __ffma2_rn(f2(w[i]), t, acc[k][i]);
+                    for (int i = 0; i < CL; i++) acc[k][i] = __ffma2_rn(f2(w[i]), t, acc[k][i]);
+                } else if (NDIM == 2) {
+                    acc[k][0] = __ffma2_rn(f2(w[dy]), u, acc[k][0]);
+                } else {
+                    acc[k][0] = __fadd2_rn(acc[k][0], u);
+                }
             }
         }
         if (cur >= 0) flush(cur);
     }
     __syncthreads();
-    region_io<3>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
+    if (ATOMIC_FLUSH) {
+        region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
+        return;
+    }
+    // deterministic: this bin's region is disjoint from every other bin of the pass
+    const int rpc = rg.R1 * rg.R2;
+    const int x_start = (org[0] + g.G[0] - g.half[0]) % g.G[0];
+    for (int row = threadIdx.x; row < CC * rpc; row += blockDim.x) {
+        const int cc = row / rpc;
+        const int r2 = row - cc * rpc;
+        const int ry = r2 % rg.R1;
+        const int rz = r2 / rg.R1;
+        const int64_t bb = b0 + cc;
+        if (bb >= batch) continue;
+        const float2 *trow = tile + cc * rg.PP + (NDIM == 3 ? rz * rg.SP + ry * rg.R0 : (NDIM == 2 ? ry * rg.SP : 0));
+        const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+        const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+        float2 *grow = grid + (bb * g.nframes + f) * g.gsize + ((int64_t)pz * g.G[1] + py) * g.G[0];
+        int px = x_start;
+        for (int rx = 0; rx < rg.R0; rx++) {
+            const float2 v = trow[rx];
+            if (v.x != 0.0f || v.y != 0.0f) grow[px] = __ffma2_rn(v, f2(inv_scale), grow[px]);
+            px = (px + 1 == g.G[0]) ? 0 : px + 1;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1170,36 +1205,50 @@ static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float
     return DMR_OK;
 }
 
-// 3D gridding with the slab kernel: CC = min(32, pow2 >= batch) coils, NR = 32 / CC
-// row groups (capped at W; extra lanes idle)
-template <int W, int NR>
+// Gridding with the slab kernel: CC = pow2 >= batch (at most 32) coils per
+// block, NR = 32 / CC tap groups (extra lanes idle). Atomic mode launches all
+// (chunked) work items at once; deterministic mode launches whole bins one
+// colour pass at a time.
+template <int NDIM, int W, int NR, bool ATOMIC>
 static int launch_grid_slab_nr(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                                const float *weight, int wpb, int l, const Region &rg, size_t smem,
                                cudaStream_t st)
 {
-    auto kern = grid_slab_kernel<W, NR>;
+    auto kern = grid_slab_kernel<NDIM, W, NR, ATOMIC>;
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t chunks = ceil_div(batch, 1ll << l);
     DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
-    kern<<<dim3(p->nwork, (unsigned)chunks), 32 * W, smem, st>>>(
-        p->g, rg, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid, batch,
-        weight, wpb, (float)(1.0 / p->scale), l);
-    DMR_LAUNCHED("grid_slab_kernel");
+    const float inv = (float)(1.0 / p->scale);
+    if (ATOMIC) {
+        kern<<<dim3(p->nwork, (unsigned)chunks), 32 * W, smem, st>>>(
+            p->g, rg, p->work, p->scoord[0], p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid, batch,
+            weight, wpb, inv, l);
+        DMR_LAUNCHED("grid_slab_kernel");
+        return DMR_OK;
+    }
+    for (size_t c = 0; c + 1 < p->det_color_start.size(); c++) {
+        const int n = p->det_color_start[c + 1] - p->det_color_start[c];
+        if (n == 0) continue;
+        kern<<<dim3(n, (unsigned)chunks), 32 * W, smem, st>>>(
+            p->g, rg, p->det_work + p->det_color_start[c], p->scoord[0], p->scoord[1], p->scoord[2], p->sidx,
+            ksp, kreal, grid, batch, weight, wpb, inv, l);
+        DMR_LAUNCHED("grid_slab_kernel");
+    }
     return DMR_OK;
 }
 
-template <int NDIM, int W>
+template <int NDIM, int W, bool ATOMIC>
 static int launch_grid_slab(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                             const float *weight, int wpb, cudaStream_t st)
 {
-    using S = CubeShape<3, W>;
+    using S = CubeShape<NDIM, W>;
     const size_t limit = (size_t)max_smem();
     int l = 0;
     while ((1ll << l) < batch && l < 5) l++;
     Region rg;
     size_t smem = 0;
     for (; l >= 0; l--) {
-        rg = cube_region<3, W>(p->g, 1 << l);
+        rg = cube_region<NDIM, W>(p->g, 1 << l);
         smem = S::meta_bytes() + (size_t)(1 << l) * rg.PP * sizeof(float2);
         if (smem <= limit) break;
     }
@@ -1207,12 +1256,12 @@ static int launch_grid_slab(const dmr_plan *p, const void *ksp, int kreal, float
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->nwork == 0) return DMR_OK;
     switch (l) {
-    case 5: return launch_grid_slab_nr<W, 1>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
-    case 4: return launch_grid_slab_nr<W, 2>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
-    case 3: return launch_grid_slab_nr<W, 4>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
-    case 2: return launch_grid_slab_nr<W, 8>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
-    case 1: return launch_grid_slab_nr<W, 16>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
-    default: return launch_grid_slab_nr<W, 32>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 5: return launch_grid_slab_nr<NDIM, W, 1, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 4: return launch_grid_slab_nr<NDIM, W, 2, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 3: return launch_grid_slab_nr<NDIM, W, 4, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 2: return launch_grid_slab_nr<NDIM, W, 8, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    case 1: return launch_grid_slab_nr<NDIM, W, 16, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
+    default: return launch_grid_slab_nr<NDIM, W, 32, ATOMIC>(p, ksp, kreal, grid, batch, weight, wpb, l, rg, smem, st);
     }
 }
 
@@ -1303,16 +1352,16 @@ int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, i
                   const float *weight, int wpb, int det, cudaStream_t st)
 {
     const int cw = cube_width(p->g);
-    if (!det && cw > 0 && p->g.ndim == 3 && grid_variant() == 1) {
-        switch (cw) {
-        case 1: return launch_grid_slab<3, 1>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 2: return launch_grid_slab<3, 2>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 3: return launch_grid_slab<3, 3>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 4: return launch_grid_slab<3, 4>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 5: return launch_grid_slab<3, 5>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 6: return launch_grid_slab<3, 6>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 7: return launch_grid_slab<3, 7>(p, ksp, kreal, grid, batch, weight, wpb, st);
-        case 8: return launch_grid_slab<3, 8>(p, ksp, kreal, grid, batch, weight, wpb, st);
+    if (cw > 0 && (det || (p->g.ndim == 3 && grid_variant() == 1))) {
+        switch (p->g.ndim * 100 + cw) {
+#define SLAB(N, W)                                                                                  \
+    case N * 100 + W:                                                                               \
+        return det ? launch_grid_slab<N, W, false>(p, ksp, kreal, grid, batch, weight, wpb, st)     \
+                   : launch_grid_slab<N, W, true>(p, ksp, kreal, grid, batch, weight, wpb, st);
+            SLAB(1, 1) SLAB(1, 2) SLAB(1, 3) SLAB(1, 4) SLAB(1, 5) SLAB(1, 6) SLAB(1, 7) SLAB(1, 8)
+            SLAB(2, 1) SLAB(2, 2) SLAB(2, 3) SLAB(2, 4) SLAB(2, 5) SLAB(2, 6) SLAB(2, 7) SLAB(2, 8)
+            SLAB(3, 1) SLAB(3, 2) SLAB(3, 3) SLAB(3, 4) SLAB(3, 5) SLAB(3, 6) SLAB(3, 7) SLAB(3, 8)
+#undef SLAB
         default: break;
         }
     }
