@@ -809,10 +809,16 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
         region_io<NDIM>(g, rg, org, f, b0, CC, batch, tile, grid, true, inv_scale);
         return;
     }
-    // deterministic: this bin's region is disjoint from every other bin of the pass
+    // deterministic: this bin's region is disjoint from every other bin of the
+    // pass. A region longer than the grid on some axis (tiny grids) wraps onto
+    // itself: then a single thread adds it, in a fixed order.
+    const bool self_alias = rg.R0 > g.G[0] || (NDIM > 1 && rg.R1 > g.G[1]) || (NDIM > 2 && rg.R2 > g.G[2]);
+    if (self_alias && threadIdx.x != 0) return;
     const int rpc = rg.R1 * rg.R2;
     const int x_start = (org[0] + g.G[0] - g.half[0]) % g.G[0];
-    for (int row = threadIdx.x; row < CC * rpc; row += blockDim.x) {
+    const int rstart = self_alias ? 0 : threadIdx.x;
+    const int rstep = self_alias ? 1 : blockDim.x;
+    for (int row = rstart; row < CC * rpc; row += rstep) {
         const int cc = row / rpc;
         const int r2 = row - cc * rpc;
         const int ry = r2 % rg.R1;
