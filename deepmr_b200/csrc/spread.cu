@@ -1250,7 +1250,9 @@ static int launch_grid_slab(const dmr_plan *p, const void *ksp, int kreal, float
     using S = CubeShape<NDIM, W>;
     const size_t limit = (size_t)max_smem();
     int l = 0;
-    while ((1ll << l) < batch && l < 5) l++;
+    // deterministic passes run whole (unsplit) bins: at most 8 coils per block
+    // so a dense bin is shared by several blocks (one per coil chunk)
+    while ((1ll << l) < batch && l < (ATOMIC ? 5 : 3)) l++;
     Region rg;
     size_t smem = 0;
     for (; l >= 0; l--) {
