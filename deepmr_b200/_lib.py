@@ -39,6 +39,7 @@ SYMBOLS = (
     "dmr_nufft_workspace_bytes",
     "dmr_nufft_forward",
     "dmr_nufft_adjoint",
+    "dmr_nufft_traj_grad",
     "dmr_toeplitz_workspace_bytes",
     "dmr_toeplitz_finalize",
     "dmr_toeplitz_apply",
@@ -87,6 +88,10 @@ _SIGS = {
     "dmr_nufft_adjoint": (
         ctypes.c_int,
         [vp, vp, ctypes.c_int, vp, i64, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t, vp],
+    ),
+    "dmr_nufft_traj_grad": (
+        ctypes.c_int,
+        [vp, vp, ctypes.c_int, vp, i64, vp, ctypes.c_int, ctypes.c_double, vp, vp, ctypes.c_size_t, vp],
     ),
     "dmr_toeplitz_workspace_bytes": (ctypes.c_int, [ctypes.c_int, i32p, i64, szp]),
     "dmr_toeplitz_finalize": (

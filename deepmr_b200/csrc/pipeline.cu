@@ -295,12 +295,14 @@ extern "C" int dmr_nufft_workspace_bytes(dmr_plan *p, int64_t batch, size_t *byt
     return nufft_ws(p, batch, nullptr, 0, w, bytes);
 }
 
-extern "C" int dmr_nufft_forward(dmr_plan *p, const void *image, int image_real, void *kspace,
-                                 int64_t batch, const float *weight, int weight_per_batch,
-                                 void *workspace, size_t workspace_bytes, void *stream)
+namespace dmr {
+
+// workspace carve + apodise/zero-pad/ifftshift + forward cuFFT: the grid of
+// the forward NUFFT (FFT order), shared by the forward and the trajectory
+// gradient
+int forward_grid(dmr_plan *p, const void *image, int image_real, int64_t batch, void *workspace,
+                 size_t workspace_bytes, cudaStream_t st, float2 **grid_out)
 {
-    DMR_CHECK(p && image && kspace && batch >= 1, DMR_ERR_INVALID, "bad argument");
-    cudaStream_t st = (cudaStream_t)stream;
     const Geom &g = p->g;
     NufftWs w;
     DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
@@ -322,7 +324,21 @@ extern "C" int dmr_nufft_forward(dmr_plan *p, const void *image, int image_real,
     r.in_real = image_real;
     DMR_TRY(launch_resize(r, image, w.grid, st));
     DMR_TRY(fft_exec(*w.fft, w.grid, CUFFT_FORWARD, w.fft_work, st));
-    return interp_dispatch(p, w.grid, (float2 *)kspace, batch, weight, weight_per_batch, st);
+    *grid_out = w.grid;
+    return DMR_OK;
+}
+
+}  // namespace dmr
+
+extern "C" int dmr_nufft_forward(dmr_plan *p, const void *image, int image_real, void *kspace,
+                                 int64_t batch, const float *weight, int weight_per_batch,
+                                 void *workspace, size_t workspace_bytes, void *stream)
+{
+    DMR_CHECK(p && image && kspace && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    float2 *grid = nullptr;
+    DMR_TRY(forward_grid(p, image, image_real, batch, workspace, workspace_bytes, st, &grid));
+    return interp_dispatch(p, grid, (float2 *)kspace, batch, weight, weight_per_batch, st);
 }
 
 extern "C" int dmr_nufft_adjoint(dmr_plan *p, const void *kspace, int kspace_real, void *image,

@@ -341,7 +341,7 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     DMR_TRY(dev_alloc(&counts, nkeys));
     tmp.ptr[3] = counts;
     DMR_TRY(dev_alloc(&d_foff, nframes + 1));
-    tmp.ptr[4] = d_foff;
+    p->foff_dev = d_foff;  // kept by the plan
     DMR_TRY(dev_alloc(&d_err, 1));
     tmp.ptr[5] = d_err;
     for (int a = 0; a < ndim; a++) {

@@ -69,6 +69,7 @@ struct dmr_plan {
     dmr::WorkItem *det_work = nullptr;
     std::vector<int> det_color_start;   // host, ncolors + 1
     float *apod[3] = {nullptr, nullptr, nullptr};  // per-axis apodisation (image index)
+    int64_t *foff_dev = nullptr;        // frame offsets on the device (nframes + 1)
 
     ~dmr_plan()
     {
@@ -81,5 +82,6 @@ struct dmr_plan {
         cudaFree(work);
         cudaFree(tiles);
         cudaFree(det_work);
+        cudaFree(foff_dev);
     }
 };

@@ -4,6 +4,8 @@ One-shot ``nufft`` / ``nufft_adj`` (reference: src/deepmr/fft/__init__.py:145-28
 and the plan/apply functions of ``deepmr.fft.nufft``.
 """
 
+import torch
+
 from . import nufft as _nufft
 from . import toeplitz as _toeplitz
 from .nufft import (  # noqa: F401
@@ -14,6 +16,7 @@ from .nufft import (  # noqa: F401
     plan_nufft,
     plan_toeplitz_nufft,
 )
+from .nufft import traj_grad  # noqa: F401
 from .toeplitz import GramMatrix  # noqa: F401
 
 __all__ = [
@@ -28,6 +31,7 @@ __all__ = [
     "GramMatrix",
     "set_deterministic_gridding",
     "deterministic_gridding",
+    "traj_grad",
 ]
 
 
@@ -60,6 +64,11 @@ def nufft(image, coord, shape=None, basis_adjoint=None, device="cpu", threadsper
     ndim = coord.shape[-1] if not isinstance(coord, (list, tuple)) else coord[0].shape[-1]
     if shape is None:
         shape = image.shape[-ndim:]
+    if isinstance(coord, torch.Tensor) and coord.requires_grad and torch.is_grad_enabled():
+        # differentiable w.r.t. the trajectory as well (extension)
+        if basis_adjoint is not None:
+            raise NotImplementedError("trajectory gradient with a low-rank basis")
+        return _nufft.NUFFTTraj.apply(_nufft._as_cfloat(image), coord, shape, width, oversamp, device, None)
     plan = _nufft.plan_nufft(coord, shape, width, oversamp, device)
     return _nufft.apply_nufft(image, plan, basis_adjoint, threadsperblock=threadsperblock)
 
@@ -67,5 +76,9 @@ def nufft(image, coord, shape=None, basis_adjoint=None, device="cpu", threadsper
 def nufft_adj(kspace, coord, shape, basis=None, device="cpu", threadsperblock=128, width=4,
               oversamp=1.25):
     """N-dimensional adjoint NUFFT, plan + apply (reference: src/deepmr/fft/__init__.py:221-286)."""
+    if isinstance(coord, torch.Tensor) and coord.requires_grad and torch.is_grad_enabled():
+        if basis is not None:
+            raise NotImplementedError("trajectory gradient with a low-rank basis")
+        return _nufft.NUFFTAdjTraj.apply(_nufft._as_cfloat(kspace), coord, shape, width, oversamp, device, None)
     plan = _nufft.plan_nufft(coord, shape, width, oversamp, device)
     return _nufft.apply_nufft_adj(kspace, plan, basis, threadsperblock=threadsperblock)

@@ -479,3 +479,80 @@ def _apply_nufft_selfadj(image, toeplitz_kern, device, threadsperblock):
         toeplitz_kern.to(device)
     out = _toeplitz.apply_toeplitz(image, toeplitz_kern)
     return out.numpy(force=True) if isnumpy else out
+
+
+# ---------------------------------------------------------------------------
+# differentiation w.r.t. the trajectory (no counterpart in the reference,
+# whose plan is an opaque object and whose backward returns no coordinate
+# gradient, nufft.py:188-209)
+# ---------------------------------------------------------------------------
+def traj_grad(nufft_plan, image, v, weight=None, post_scale=1.0):
+    """g[..., a] = post_scale * sum_batch Re(conj(v) * d apply_nufft(image) / d coord[..., a]).
+
+    Returns a float32 tensor shaped like the plan's coordinates
+    ``(ncontrasts, nviews, nsamples, ndim)`` (flat ``(total, ndim)`` for
+    uneven frames), in grid units.
+    """
+    interp = nufft_plan.interpolator
+    dev = interp.device
+    ndim = nufft_plan.ndim
+    x = _as_cfloat(image).to(dev).contiguous()
+    vv = torch.as_tensor(v).to(dev, torch.complex64).contiguous()
+    nframes = interp.nframes
+    batch_shape = x.shape[:-ndim] if nframes == 1 else x.shape[: -ndim - 1]
+    frames_shape = () if nframes == 1 else (nframes,)
+    batch = int(np.prod(batch_shape))
+    out = torch.empty((interp.total, ndim), dtype=torch.float32, device=dev)
+    w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+    ws = interp.workspace(batch)
+    with torch.cuda.device(dev):
+        _lib.check(_lib.lib().dmr_nufft_traj_grad(
+            interp.handle, _lib.ptr(x), int(not x.is_complex()), _lib.ptr(vv), batch, _lib.ptr(w), wpb,
+            float(post_scale), _lib.ptr(out), _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev)))
+    return out
+
+
+class NUFFTTraj(autograd.Function):
+    """y = A(coord) x with gradients for the image (the reference's adjoint
+    convention, nufft.py:188-209) and for the coordinates."""
+
+    @staticmethod
+    def forward(ctx, image, coord, shape, width, oversamp, device, weight):
+        plan = plan_nufft(coord.detach(), shape, width, oversamp, device)
+        ctx.plan, ctx.weight, ctx.coord_shape = plan, weight, coord.shape
+        ctx.save_for_backward(image)
+        return _apply_nufft(image.detach(), plan, None, weight, None, 128)
+
+    @staticmethod
+    def backward(ctx, g):
+        (image,) = ctx.saved_tensors
+        gx = gc = None
+        if ctx.needs_input_grad[0]:
+            gx = _apply_nufft_adj(g, ctx.plan, None, ctx.weight, None, 128).to(image.device)
+        if ctx.needs_input_grad[1]:
+            gc = traj_grad(ctx.plan, image.detach(), g, ctx.weight).reshape(ctx.coord_shape)
+        return gx, gc, None, None, None, None, None
+
+
+class NUFFTAdjTraj(autograd.Function):
+    """x = A(coord)^H y (reference scale: exact adjoint / prod(os_shape)) with
+    gradients for the k-space data and for the coordinates."""
+
+    @staticmethod
+    def forward(ctx, kspace, coord, shape, width, oversamp, device, weight):
+        plan = plan_nufft(coord.detach(), shape, width, oversamp, device)
+        ctx.plan, ctx.weight, ctx.coord_shape = plan, weight, coord.shape
+        ctx.save_for_backward(kspace)
+        return _apply_nufft_adj(kspace.detach(), plan, None, weight, None, 128)
+
+    @staticmethod
+    def backward(ctx, g):
+        (kspace,) = ctx.saved_tensors
+        gy = gc = None
+        if ctx.needs_input_grad[0]:
+            gy = _apply_nufft(g, ctx.plan, None, ctx.weight, None, 128).to(kspace.device)
+        if ctx.needs_input_grad[1]:
+            G = float(np.prod([int(s) for s in ctx.plan.os_shape]))
+            gc = traj_grad(ctx.plan, g, kspace.detach(), ctx.weight, 1.0 / G).reshape(ctx.coord_shape)
+        return gy, gc, None, None, None, None, None
+

@@ -160,6 +160,24 @@ int dmr_nufft_adjoint(dmr_plan *plan, const void *kspace, int kspace_real,
                       int weight_per_batch, int deterministic,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/*
+ * Trajectory gradient of the NUFFT. No counterpart in the reference: its
+ * autograd returns no coordinate gradient (src/deepmr/fft/nufft.py:188-209).
+ *   grad[p, a] = post_scale * sum_b Re(conj(v_b[p]) * dy_b[p] / dcoord[p, a])
+ * where y = dmr_nufft_forward(image) with `weight` (derivative of the
+ * Kaiser-Bessel weights with the tap set held fixed; 0 on Cartesian axes).
+ *  image: (batch, nframes, *shape) complex64 (float32 if image_real);
+ *  v: (batch, total) complex64; grad: (total, ndim) float32 in the original
+ *  sample order, coordinate axes (x, y, z), fully written (deterministic).
+ * Forward operator y = A x: image = x, v = dL/dy, post_scale = 1.
+ * Adjoint operator x = A^H y: image = dL/dx, v = y, post_scale = 1/prod(os_shape).
+ * Uses the forward NUFFT workspace (dmr_nufft_workspace_bytes). Widths <= 8.
+ */
+int dmr_nufft_traj_grad(dmr_plan *plan, const void *image, int image_real,
+                        const void *v, int64_t batch, const float *weight,
+                        int weight_per_batch, double post_scale, float *grad,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
 /* Bytes of workspace dmr_toeplitz_apply / dmr_toeplitz_finalize need. */
 int dmr_toeplitz_workspace_bytes(int ndim, const int32_t *kshape,
                                  int64_t batch, size_t *bytes);

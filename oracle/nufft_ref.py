@@ -433,3 +433,73 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.complex128).ravel()
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+# --------------------------------------------------------------------------
+# float64 forward (finite-difference reference for the gradient tests): the
+# reference's forward (nufft.py:450-528) with every step in float64; the
+# oversampled spectrum is computed once and samples are evaluated on demand
+# --------------------------------------------------------------------------
+class Forward64:
+    """y[..., p] = (1/scale) sum_taps prod KB * K[taps] in float64."""
+
+    def __init__(self, image, coord, shape, width=4, oversamp=1.25):
+        import itertools
+
+        self._product = itertools.product
+        coord = np.asarray(coord, dtype=np.float32)
+        self.ndim = ndim = coord.shape[-1]
+        self.plan = plan = plan_nufft(torch.as_tensor(coord), shape, width, oversamp)
+        x = torch.as_tensor(np.asarray(image, dtype=np.complex128)).clone()
+        for n in range(1, ndim + 1):
+            axis = -n
+            if plan.width[axis] == 1:
+                continue
+            i = x.shape[axis]
+            os_i = math.ceil(float(plan.oversamp[axis]) * i)
+            idx = torch.arange(i, dtype=torch.float64)
+            b = float(plan.beta[axis])
+            ap = (b**2 - (math.pi * int(plan.width[axis]) * (idx - i // 2) / os_i) ** 2) ** 0.5
+            ap = ap / torch.sinh(ap)
+            ap = torch.nan_to_num(ap / ap[i // 2], nan=1.0)
+            x = x * ap.reshape([i] + [1] * (-axis - 1))
+        os_shape = [int(s) for s in plan.os_shape]
+        x = resize(x, list(x.shape[:-ndim]) + os_shape)
+        self.K = centered_fft(x, ndim, norm=None).numpy()
+        self.scale = plan.interpolator.scale
+        self.width_xyz = [int(w) for w in plan.width][::-1]
+        self.beta_xyz = [float(b) for b in plan.beta][::-1]
+        self.G_xyz = os_shape[::-1]
+        self.N_xyz = [int(s) for s in plan.shape][::-1]
+        self.os_xyz = [float(o) for o in plan.oversamp][::-1]
+
+    def rescaled(self, c):
+        """Rescaled (grid-index) coordinates of one sample, float64."""
+        out = []
+        for a in range(self.ndim):
+            g = math.ceil(self.os_xyz[a] * self.N_xyz[a])
+            out.append(float(c[a]) * g / self.N_xyz[a] + g // 2)
+        return out
+
+    def sample(self, c):
+        """y[..., one sample] at coordinates c (grid units, (x, y, z))."""
+        taps, wts = [], []
+        for a, k in enumerate(self.rescaled(c)):
+            W = self.width_xyz[a]
+            G = self.G_xyz[a]
+            if W == 1:
+                taps.append([int(k) % G])
+                wts.append([1.0])
+                continue
+            x0 = math.ceil(k - W / 2)
+            taps.append([(x0 + i) % G for i in range(W)])
+            wts.append([kaiser_bessel(((x0 + i) - k) / (W / 2), self.beta_xyz[a]) for i in range(W)])
+        acc = np.zeros(self.K.shape[:-self.ndim], dtype=np.complex128)
+        for combo in self._product(*[range(len(t)) for t in taps]):
+            w = 1.0
+            index = []
+            for a, i in enumerate(combo):
+                w *= wts[a][i]
+                index.append(taps[a][i])
+            acc = acc + w * self.K[(...,) + tuple(index[::-1])]
+        return acc / self.scale
