@@ -16,6 +16,7 @@ from .nufft import (  # noqa: F401
     plan_nufft,
     plan_toeplitz_nufft,
 )
+from .graphs import CapturedNUFFT, frames_concat, frames_split  # noqa: F401
 from .nufft import traj_grad  # noqa: F401
 from .toeplitz import GramMatrix  # noqa: F401
 
@@ -32,6 +33,9 @@ __all__ = [
     "set_deterministic_gridding",
     "deterministic_gridding",
     "traj_grad",
+    "CapturedNUFFT",
+    "frames_split",
+    "frames_concat",
 ]
 
 

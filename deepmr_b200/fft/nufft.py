@@ -238,6 +238,10 @@ def plan_nufft(coord, shape, width=4, oversamp=1.25, device="cpu", tile=None):
     oversamp[is_cart] = 1.0
     width[is_cart] = 1
     os_shape = np.ceil(oversamp * shape).astype(np.int16)
+    if tile is None:
+        from .. import autotune
+
+        tile = autotune.lookup(ndim, int(width.max()), float(oversamp.max()))
 
     interp = DevicePlan(flat, offs, ishape, ndim, shape, os_shape, width, beta, oversamp, dev, tile)
     return NUFFTPlan(ndim, tuple(oversamp), tuple(width), tuple(beta), tuple(os_shape),
@@ -383,6 +387,13 @@ def _sample_shape(interp):
     return interp.ishape if interp.ishape is not None else (interp.total,)
 
 
+def _kspace_shape(interp, batch_shape):
+    """k-space layout: (..., [F,] nviews, nsamples), or (..., total) for uneven frames."""
+    if interp.ishape is None:
+        return list(batch_shape) + [interp.total]
+    return list(batch_shape) + ([interp.nframes] if interp.nframes > 1 else []) + list(interp.ishape)
+
+
 def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
     """Returns (tensor, per_batch flag) for the C library's weight argument."""
     if weight is None:
@@ -390,8 +401,7 @@ def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
     w = torch.as_tensor(weight, dtype=torch.float32).to(dev)
     if w.numel() == interp.total:
         return w.contiguous(), 0
-    full = list(batch_shape) + list(frames_shape) + list(_sample_shape(interp))
-    return torch.broadcast_to(w, full).contiguous(), 1
+    return torch.broadcast_to(w, _kspace_shape(interp, batch_shape)).contiguous(), 1
 
 
 def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblock):
@@ -417,8 +427,7 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
         raise ValueError(f"image spatial shape {tuple(x.shape[-ndim:])} != plan shape {nufft_plan.shape}")
     batch = int(np.prod(batch_shape))
     x = x.contiguous()
-    out = torch.empty(list(batch_shape) + list(frames_shape) + list(_sample_shape(interp)),
-                      dtype=torch.complex64, device=dev)
+    out = torch.empty(_kspace_shape(interp, batch_shape), dtype=torch.complex64, device=dev)
     if batch > 0 and interp.total > 0:
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
         ws = interp.workspace(batch)
@@ -445,13 +454,12 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock)
     nframes = interp.nframes
     y = kspace.to(dev)
     nsd = _sample_dims(interp)
-    if nframes == 1:
+    frames_shape = (nframes,) if nframes > 1 else ()
+    if nframes == 1 or interp.ishape is None:
         batch_shape = y.shape[:-nsd]
-        frames_shape = ()
     else:
         batch_shape = y.shape[: -nsd - 1]
-        frames_shape = (nframes,)
-    if tuple(y.shape[len(batch_shape) + len(frames_shape):]) != tuple(_sample_shape(interp)):
+    if list(y.shape) != _kspace_shape(interp, batch_shape):
         raise ValueError(f"kspace shape {tuple(y.shape)} does not match the plan samples {_sample_shape(interp)}")
     batch = int(np.prod(batch_shape))
     y = y.contiguous()
