@@ -85,7 +85,7 @@ def _time(fn, repeats):
     return a.elapsed_time(b) / repeats
 
 
-def tune(ndim, width, oversamp, repeats=5, save=True, verbose=True):
+def tune(ndim, width, oversamp, repeats=5, save=True, verbose=True, out=None):
     """Time each candidate bin and record the fastest; returns (tile, timings)."""
     import deepmr_b200.fft as F
     from . import synth
@@ -110,7 +110,7 @@ def tune(ndim, width, oversamp, repeats=5, save=True, verbose=True):
             "workload": f"{ndim}D n={n} coils={coils} radial, forward+adjoint",
             "device": torch.cuda.get_device_name(),
         }
-        with open(TABLE_PATH, "w") as f:
+        with open(out or TABLE_PATH, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
     return best, timings
 
@@ -121,12 +121,13 @@ def main():
     ap.add_argument("--width", type=int)
     ap.add_argument("--oversamp", type=float)
     ap.add_argument("--all", action="store_true", help="the benchmark configurations")
+    ap.add_argument("--out", help="table path (default: the package table)")
     a = ap.parse_args()
     if a.all:
         for cfg in [(2, 3, 2.0), (2, 4, 1.25), (2, 6, 2.0), (3, 4, 1.25), (3, 6, 2.0), (1, 4, 1.25)]:
-            tune(*cfg)
+            tune(*cfg, out=a.out)
     else:
-        tune(a.ndim, a.width, a.oversamp)
+        tune(a.ndim, a.width, a.oversamp, out=a.out)
 
 
 if __name__ == "__main__":
