@@ -43,6 +43,11 @@ SYMBOLS = (
     "dmr_toeplitz_workspace_bytes",
     "dmr_toeplitz_finalize",
     "dmr_toeplitz_apply",
+    "dmr_sense_normal",
+    "dmr_cg_state_bytes",
+    "dmr_cg_init",
+    "dmr_cg_step",
+    "dmr_cg_residual",
     "dmr_toeplitz_normalize_noalloc",
 )
 
@@ -103,6 +108,14 @@ _SIGS = {
         [ctypes.c_int, i32p, i32p, vp, i64, vp, ctypes.c_int, vp, i64, vp, ctypes.c_size_t, vp],
     ),
     "dmr_toeplitz_normalize_noalloc": (ctypes.c_int, [vp, i64, vp]),
+    "dmr_sense_normal": (
+        ctypes.c_int,
+        [ctypes.c_int, i32p, i32p, vp, vp, i64, vp, vp, ctypes.c_float, vp, ctypes.c_size_t, vp],
+    ),
+    "dmr_cg_state_bytes": (ctypes.c_int, [szp]),
+    "dmr_cg_init": (ctypes.c_int, [vp, vp, vp, vp, i64, vp, vp]),
+    "dmr_cg_step": (ctypes.c_int, [vp, vp, vp, vp, i64, vp, vp]),
+    "dmr_cg_residual": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double), vp]),
 }
 
 

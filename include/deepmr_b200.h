@@ -208,6 +208,39 @@ int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t *ishape,
                        void *workspace, size_t workspace_bytes, void *stream);
 
 /*
+ * SENSE + Toeplitz normal operator of a CG-SENSE reconstruction:
+ *   out = sum_c conj(S_c) * T(S_c * x) + lamda * x
+ * with T the Toeplitz self-adjoint of dmr_toeplitz_apply (single kernel
+ * frame). Replaces C.H * NUFFTGramOp * C (+ lamda * Identity) of
+ * src/deepmr/recon/alg/linop.py:145-146 and src/deepmr/optim/cg.py:86-94:
+ * coil expansion is fused into the zero-pad kernel and the coil sum (in coil
+ * order, deterministic) + lamda * x into the crop kernel.
+ *  kernel: (*kshape) complex64; maps: (ncoils, *ishape); x, out: (*ishape),
+ *  not aliased. Workspace: dmr_toeplitz_workspace_bytes(ndim, kshape, ncoils).
+ */
+int dmr_sense_normal(int ndim, const int32_t *kshape, const int32_t *ishape,
+                     const void *kernel, const void *maps, int64_t ncoils,
+                     const void *x, void *out, float lamda, void *workspace,
+                     size_t workspace_bytes, void *stream);
+
+/*
+ * Conjugate gradient of cg_solve / CGStep (src/deepmr/optim/cg.py:16-221)
+ * with every scalar kept on the device (no host synchronisation per step) and
+ * float64 inner products reduced in a fixed order. `state` is a device buffer
+ * of dmr_cg_state_bytes bytes. dmr_cg_init: x = 0, r = p = ahy,
+ * rsold = <r, r>. dmr_cg_step, given q = AHA(p): alpha = rsold / <p, q>,
+ * x += alpha p, r -= alpha q, rsnew = Re<r, r>, p = r + (rsnew / rsold) p.
+ * dmr_cg_residual copies rsnew to the host (synchronises the stream).
+ * All vectors are complex64 of n elements.
+ */
+int dmr_cg_state_bytes(size_t *bytes);
+int dmr_cg_init(const void *ahy, void *x, void *r, void *p, int64_t n,
+                void *state, void *stream);
+int dmr_cg_step(void *x, void *r, void *p, const void *q, int64_t n,
+                void *state, void *stream);
+int dmr_cg_residual(const void *state, double *rsnew, void *stream);
+
+/*
  * Allocation-free variant of the Toeplitz kernel normalisation step.
  * No counterpart in the reference. For callers that must not allocate device
  * memory (an application that hands the GPU a fixed memory pool at start-up,
