@@ -88,7 +88,7 @@ def test_serving_admission_respects_budget():
 
     reqs = _requests()
     server = recon.ReconServer(device="cuda", max_active=6,
-                               hbm_budget=max(recon.ReconServer().request_bytes(r) for r in reqs))
+                               hbm_budget=min(recon.ReconServer().request_bytes(r) for r in reqs))
     server.prepare(reqs)
     stats = server.run(reqs, realtime=False)
     assert stats.peak_active == 1 and len(stats.results) == len(reqs)
