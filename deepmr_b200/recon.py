@@ -24,6 +24,7 @@ what else runs beside it (bitwise).
 """
 
 import ctypes
+import importlib
 import math
 import time
 from dataclasses import dataclass, field
@@ -32,7 +33,10 @@ import numpy as np
 import torch
 
 from . import _lib
-from .fft import nufft as _nufft
+
+# the package attribute deepmr_b200.fft.nufft is the one-shot function (as in
+# the reference); take the submodule from the import system
+_nufft = importlib.import_module("deepmr_b200.fft.nufft")
 
 
 def _ws_bytes(ndim, kshape, batch, dev):
@@ -322,7 +326,8 @@ def synthetic_requests(n, rate_hz, seed=0, sizes=(128, 192, 256, 320), coils=(8,
     trajectory, random-phase Gaussian-blob coil maps (sum |S|^2 = 1),
     k-space simulated from a seeded ellipse phantom plus noise."""
     from . import synth
-    from .fft import nufft as nf
+
+    nf = _nufft
 
     rng = np.random.default_rng(seed)
     t = 0.0

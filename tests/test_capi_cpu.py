@@ -114,3 +114,15 @@ def test_public_api_fails_loudly_without_cuda():
     for call in calls:
         with pytest.raises(RuntimeError, match="CUDA"):
             call()
+
+
+def test_modules_bind_the_nufft_submodule():
+    """deepmr_b200.fft.nufft is the one-shot function (as in the reference);
+    internal users must hold the submodule."""
+    import types
+
+    from deepmr_b200 import recon
+    from deepmr_b200.fft import graphs, toeplitz  # noqa: F401
+
+    assert isinstance(recon._nufft, types.ModuleType)
+    assert callable(recon._nufft.plan_nufft)
