@@ -442,7 +442,7 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
     return out.numpy(force=True) if isnumpy else out
 
 
-def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock):
+def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock, deterministic=None):
     isnumpy = isinstance(kspace, np.ndarray)
     kspace = _as_cfloat(kspace)
     _check_basis(basis)
@@ -472,7 +472,8 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock)
             _lib.check(
                 _lib.lib().dmr_nufft_adjoint(
                     interp.handle, _lib.ptr(y), int(not y.is_complex()), _lib.ptr(out), batch,
-                    _lib.ptr(w), wpb, int(DETERMINISTIC_GRIDDING), _lib.ptr(ws), ws.numel(),
+                    _lib.ptr(w), wpb, int(DETERMINISTIC_GRIDDING if deterministic is None else deterministic),
+                    _lib.ptr(ws), ws.numel(),
                     _lib.stream_ptr(dev),
                 )
             )

@@ -118,8 +118,12 @@ class CGState:
 
 
 def sense_adjoint(kspace, plan, maps, dcf=None):
-    """AHy = sum_c conj(S_c) nufft_adj(dcf * y_c) (E^H(dcf**0.5 y), classic_recon.py:153-156)."""
-    img = _nufft.apply_nufft_adj(kspace, plan, weight=dcf)
+    """AHy = sum_c conj(S_c) nufft_adj(dcf * y_c) (E^H(dcf**0.5 y), classic_recon.py:153-156).
+
+    Gridding runs in the deterministic mode, so AHy (and the whole
+    reconstruction) is bitwise independent of concurrent work.
+    """
+    img = _nufft._apply_nufft_adj(kspace, plan, None, dcf, None, 128, deterministic=True)
     return (maps.conj() * img).sum(0)
 
 
