@@ -51,7 +51,7 @@ def plan_toeplitz(coord, shape, basis=None, dcf=None, width=6, device="cpu"):
     """Compute the Toeplitz kernel of A^H A (reference: toeplitz.py:15-157)."""
     # deferred import (nufft imports this module); import names from the
     # submodule: the package attribute `nufft` is the one-shot function
-    from .nufft import apply_nufft_adj, compute_device, detect_cartesian, plan_nufft
+    from .nufft import _apply_nufft_adj, compute_device, detect_cartesian, plan_nufft
 
     if basis is not None:
         raise NotImplementedError(
@@ -79,7 +79,8 @@ def plan_toeplitz(coord, shape, basis=None, dcf=None, width=6, device="cpu"):
     # the float64 product back to float32
     coord2 = coord * torch.as_tensor(oversamp)
     plan = plan_nufft(coord2, kshape, width, 1.25, dev)
-    psf = apply_nufft_adj(dcf * delta, plan)
+    # deterministic gridding: the kernel (planned once) is bitwise reproducible
+    psf = _apply_nufft_adj(dcf * delta, plan, None, None, None, 128, deterministic=True)
     psf = psf.to(dev).contiguous()
 
     K = [int(k) for k in kshape]
