@@ -35,6 +35,8 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(N=192, coils=32, spokes=50000, samples=384, width=4, oversamp=1.25)
 FALLBACK_HBM_GBS = 6650.0
 METRIC = "NUFFT fwd+adj k-space samples/s (3D kooshball)"
+# kernels the library launches for 3D, width 4, 32 coils (spread.cu dispatch)
+KERNELS = {"interp": "interp_cube_kernel", "grid": "grid_cube_kernel", "grid_det": "grid_slab_kernel"}
 UNIT = "samples/s"
 
 
@@ -303,10 +305,11 @@ def run_b200(args):
     torch.cuda.empty_cache()
 
     ib, gb = alg_bytes(w, M)
+    gname, iname = KERNELS["grid_det" if F.deterministic_gridding() else "grid"], KERNELS["interp"]
     if grid_ms >= interp_ms:
-        kname, kms, kbytes = "grid_atomic_kernel" if not F.deterministic_gridding() else "grid_owner_kernel", grid_ms, gb
+        kname, kms, kbytes = gname, grid_ms, gb
     else:
-        kname, kms, kbytes = "interp_kernel", interp_ms, ib
+        kname, kms, kbytes = iname, interp_ms, ib
     peak, peak_kind = measured_peak()
     achieved = kbytes / (kms / 1e3) / 1e9
     traffic = ncu_traffic(kname, w)
