@@ -36,7 +36,7 @@ WORKLOAD = dict(N=192, coils=32, spokes=50000, samples=384, width=4, oversamp=1.
 FALLBACK_HBM_GBS = 6650.0
 METRIC = "NUFFT fwd+adj k-space samples/s (3D kooshball)"
 # kernels the library launches for 3D, width 4, 32 coils (spread.cu dispatch)
-KERNELS = {"interp": "interp_cube_kernel", "grid": "grid_cube_kernel", "grid_det": "grid_slab_kernel"}
+KERNELS = {"interp": "interp_cube_kernel", "grid": "grid_cube_kernel", "grid_det": "grid_rt_kernel"}
 UNIT = "samples/s"
 
 
@@ -293,10 +293,14 @@ def run_b200(args):
     interp_ms = timed(lambda: _lib.check(L.dmr_interp(ip.handle, _lib.ptr(gbuf), _lib.ptr(kout), C, None, 0, st)), args.steps)
     grid_ms = timed(lambda: _lib.check(L.dmr_grid(ip.handle, _lib.ptr(ksp), 0, _lib.ptr(gbuf), C, _lib.ptr(dcf), 0,
                                                   int(F.deterministic_gridding()), st)), args.steps)
+    det = 1 - int(F.deterministic_gridding())
+    grid_other_ms = timed(lambda: _lib.check(L.dmr_grid(ip.handle, _lib.ptr(ksp), 0, _lib.ptr(gbuf), C, _lib.ptr(dcf),
+                                                        0, det, st)), args.steps)
     fwd_ms = timed(lambda: F.apply_nufft(img, plan), args.steps)
     adj_ms = timed(lambda: F.apply_nufft_adj(ksp, plan, weight=dcf), args.steps)
     extras = {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "interp_kernel_ms": interp_ms,
-              "grid_kernel_ms": grid_ms}
+              "grid_kernel_ms": grid_ms,
+              ("grid_deterministic_ms" if det else "grid_atomic_ms"): grid_other_ms}
     if not args.no_extras:
         T = F.plan_toeplitz_nufft(coord, N, dcf=dcf, device=dev)
         extras["toeplitz_selfadj_ms"] = timed(lambda: F.apply_nufft_selfadj(img, T), max(3, args.steps // 2))

@@ -12,7 +12,8 @@ import threading
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libdeepmr_b200.so")
+# DMR_LIBRARY selects another build of the same library (same ABI)
+LIB_PATH = os.environ.get("DMR_LIBRARY") or os.path.join(_HERE, "lib", "libdeepmr_b200.so")
 
 ERRORS = {
     -1: "DMR_ERR_INVALID",

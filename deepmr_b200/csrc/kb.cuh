@@ -44,4 +44,21 @@ inline double kb_f64(double u, double beta)
     return p * exp(a) / sqrt(a);
 }
 
+// First tap of a sample at rescaled coordinate k: ceil(k - W/2) in float64
+// (plan.py:260); truncation on a Cartesian axis (plan.py:117-121).
+__device__ __forceinline__ int first_tap_dev(float k, int W)
+{
+    if (W == 1) return (int)k;
+    return (int)ceil((double)k - 0.5 * (double)W);
+}
+
+// Kernel weight of tap i for a sample at rescaled coordinate k with first tap x0
+// (plan.py:260-268): KB(((x0 + i) - k) / (W/2)); 1 on Cartesian axes.
+__device__ __forceinline__ float tap_weight(int x0, int i, float k, int W, double inv_hw, float beta)
+{
+    if (W == 1) return 1.0f;
+    const double u = ((double)(x0 + i) - (double)k) * inv_hw;
+    return kb_f32((float)u, beta);
+}
+
 }  // namespace dmr

@@ -20,7 +20,8 @@ namespace dmr {
 int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t batch,
                     const float *weight, int wpb, cudaStream_t st);
 int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                  const float *weight, int wpb, int det, cudaStream_t st);
+                  const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
+                  cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // Generic centred resize with index rolls and per-axis apodisation:
@@ -172,6 +173,8 @@ static void zyx_dims(const Geom &g, const int *ext, int out[3])
 struct NufftWs {
     float2 *grid;
     void *fft_work;
+    void *rt_scratch;  // register-tile gridding partial sums (split regions)
+    size_t rt_bytes;
     std::shared_ptr<FftPlan> fft;
 };
 
@@ -184,13 +187,17 @@ static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, Nufft
     auto fp = get_fft_plan(g.ndim, dims, batch * g.nframes, &err);
     if (!fp) return err;
     const size_t grid_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
-    const size_t total = grid_bytes + align_up(fp->work_bytes, 256);
+    const size_t fft_bytes = align_up(fp->work_bytes, 256);
+    const size_t rt_bytes = align_up(rt_scratch_bytes(p, batch), 256);
+    const size_t total = grid_bytes + fft_bytes + rt_bytes;
     if (need) *need = total;
     if (!ws) return DMR_OK;
     DMR_CHECK(ws_bytes >= total, DMR_ERR_WORKSPACE, "workspace too small: %zu < %zu", ws_bytes, total);
     DMR_CHECK(((uintptr_t)ws & 255) == 0, DMR_ERR_INVALID, "workspace must be 256-byte aligned");
     out.grid = (float2 *)ws;
     out.fft_work = fp->work_bytes ? (char *)ws + grid_bytes : nullptr;
+    out.rt_scratch = rt_bytes ? (char *)ws + grid_bytes + fft_bytes : nullptr;
+    out.rt_bytes = rt_bytes;
     out.fft = fp;
     return DMR_OK;
 }
@@ -352,7 +359,7 @@ extern "C" int dmr_nufft_adjoint(dmr_plan *p, const void *kspace, int kspace_rea
     NufftWs w;
     DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
     DMR_TRY(grid_dispatch(p, kspace, kspace_real, w.grid, batch, weight, weight_per_batch,
-                          deterministic, st));
+                          deterministic, w.rt_scratch, w.rt_bytes, st));
     DMR_TRY(fft_exec(*w.fft, w.grid, CUFFT_INVERSE, w.fft_work, st));
     ResizeArgs r;
     memset(&r, 0, sizeof(r));

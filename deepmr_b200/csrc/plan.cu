@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -66,7 +67,7 @@ __global__ void preprocess_kernel(Geom g, const float *__restrict__ coord,
                                   float h0, float h1, float h2, float *__restrict__ rk0,
                                   float *__restrict__ rk1, float *__restrict__ rk2,
                                   int32_t *__restrict__ keys, int32_t *__restrict__ vals,
-                                  int32_t *__restrict__ counts, int *__restrict__ err)
+                                  int32_t *__restrict__ counts, int *__restrict__ err, int cell_order)
 {
     const float sc[3] = {s0, s1, s2};
     const float sh[3] = {h0, h1, h2};
@@ -91,10 +92,11 @@ __global__ void preprocess_kernel(Geom g, const float *__restrict__ coord,
             b[a] = x0m / g.T[a];
             l[a] = x0m - b[a] * g.T[a];
         }
-        // sort key: (frame, bin, cell of the first tap inside the bin)
+        // sort key: (frame, bin, cell of the first tap inside the bin), or
+        // (frame, bin) with the samples of a bin in acquisition order
         const int bin = lo * g.nbins + (b[2] * g.nb[1] + b[1]) * g.nb[0] + b[0];
         const int cell = (l[2] * g.T[1] + l[1]) * g.T[0] + l[0];
-        keys[i] = bin * (g.T[0] * g.T[1] * g.T[2]) + cell;
+        keys[i] = cell_order ? bin * (g.T[0] * g.T[1] * g.T[2]) + cell : bin;
         vals[i] = (int32_t)i;
         atomicAdd(&counts[bin], 1);
     }
@@ -355,12 +357,17 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     DMR_CUDA(cudaMemcpyAsync(d_foff, frame_offsets, (nframes + 1) * sizeof(int64_t),
                              cudaMemcpyHostToDevice, st));
 
+    // Within a bin, samples are sorted by the cell of their first tap (register
+    // reuse of the cube kernels); DMR_SORT_CELL=0 keeps them in acquisition
+    // order instead (tuning).
+    const char *env_order = getenv("DMR_SORT_CELL");
+    const int cell_order = env_order ? atoi(env_order) != 0 : 1;
     if (total > 0) {
         preprocess_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
             g, coord, d_foff, sc[0], sc[1], sc[2], sh[0], sh[1], sh[2], rk[0], rk[1], rk[2],
-            keys, vals, counts, d_err);
+            keys, vals, counts, d_err, cell_order);
         DMR_LAUNCHED("preprocess_kernel");
-        const int64_t nsort = nkeys * (int64_t)g.T[0] * g.T[1] * g.T[2];
+        const int64_t nsort = nkeys * (cell_order ? (int64_t)g.T[0] * g.T[1] * g.T[2] : 1);
         int end_bit = 1;
         while ((1ll << end_bit) < nsort) end_bit++;
         size_t temp_bytes = 0;
@@ -493,6 +500,7 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     DMR_CUDA(cudaMemcpyAsync(p->tiles, order.data(), order.size() * sizeof(int32_t),
                              cudaMemcpyHostToDevice, st));
     DMR_CUDA(cudaStreamSynchronize(st));
+    DMR_TRY(rt_build(p.get(), h_start, st));
     *out = p.release();
     return DMR_OK;
 }

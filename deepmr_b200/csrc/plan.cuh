@@ -29,6 +29,8 @@ struct Geom {
     int64_t gsize;  // grid points per (batch, frame)
     int64_t isize;  // image points per (batch, frame)
     int64_t total;  // samples over all frames
+    int nr[3];      // register-tile gridding: block regions per axis (0: not planned)
+    int nregions;   // block regions per frame
 };
 
 // One block-level unit of interpolation / atomic-gridding work: a chunk of
@@ -39,6 +41,18 @@ struct WorkItem {
     int end;
 };
 
+// One block of register-tile gridding: part `begin` of `end` equal fractions
+// of every window bin of block region `region` (frame included). slot < 0:
+// the block writes the grid; otherwise it writes partial sums to scratch slot
+// `slot`. A reduction item (region, first slot, end slot) sums the slots of a
+// split region in order.
+struct RtItem {
+    int region;
+    int begin;
+    int end;
+    int slot;
+};
+
 struct FftPlan {
     cufftHandle handle = 0;
     size_t work_bytes = 0;
@@ -47,6 +61,14 @@ struct FftPlan {
 
 // Process-wide cache of cuFFT plans keyed by (device, rank, dims, batch).
 std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t batch, int *err);
+
+// Register-tile gridding: whether the geometry admits it (3D, grid at least
+// a block region plus the kernel support on every axis); plan the block items after the bin sort (host
+// bin offsets h_start, nframes * nbins + 1 entries); scratch bytes a call of
+// `batch` coils needs (0 when the kernel does not apply).
+bool rt_geometry_ok(const Geom &g);
+int rt_build(::dmr_plan *p, const std::vector<int32_t> &h_start, cudaStream_t st);
+size_t rt_scratch_bytes(const ::dmr_plan *p, int64_t batch);
 
 }  // namespace dmr
 
@@ -70,6 +92,13 @@ struct dmr_plan {
     std::vector<int> det_color_start;   // host, ncolors + 1
     float *apod[3] = {nullptr, nullptr, nullptr};  // per-axis apodisation (image index)
     int64_t *foff_dev = nullptr;        // frame offsets on the device (nframes + 1)
+    // register-tile gridding (3D): block items, reduction items for regions
+    // split over several blocks, and the number of partial-sum slots
+    dmr::RtItem *rt_items = nullptr;
+    int nrt = 0;
+    dmr::RtItem *rt_reduce = nullptr;
+    int nrt_reduce = 0;
+    int rt_slots = 0;
 
     ~dmr_plan()
     {
@@ -83,5 +112,7 @@ struct dmr_plan {
         cudaFree(tiles);
         cudaFree(det_work);
         cudaFree(foff_dev);
+        cudaFree(rt_items);
+        cudaFree(rt_reduce);
     }
 };

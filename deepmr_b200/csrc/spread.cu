@@ -22,21 +22,6 @@
 
 namespace dmr {
 
-__device__ __forceinline__ int first_tap_dev(float k, int W)
-{
-    if (W == 1) return (int)k;  // Cartesian axis: truncation (plan.py:117-121)
-    return (int)ceil((double)k - 0.5 * (double)W);
-}
-
-// Kernel weight of tap i for a sample at rescaled coordinate k with first tap x0
-// (plan.py:260-268): KB(((x0 + i) - k) / (W/2)); 1 on Cartesian axes.
-__device__ __forceinline__ float tap_weight(int x0, int i, float k, int W, double inv_hw, float beta)
-{
-    if (W == 1) return 1.0f;
-    const double u = ((double)(x0 + i) - (double)k) * inv_hw;
-    return kb_f32((float)u, beta);
-}
-
 template <int NDIM, int WMAX>
 struct Meta {
     // samples staged per batch (sized so the weight table stays ~12 KB)
@@ -1356,9 +1341,19 @@ int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t 
     return DMR_ERR_UNSUPPORTED;
 }
 
+int grid_rt_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                     const float *weight, int wpb, void *scratch, size_t scratch_bytes, cudaStream_t st);
+
 int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                  const float *weight, int wpb, int det, cudaStream_t st)
+                  const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
+                  cudaStream_t st)
 {
+    // deterministic 3D gridding of 8+ coils: register tiles (one owner per grid
+    // point, no colour passes) when the plan has them
+    if (det) {
+        const int rc = grid_rt_dispatch(p, ksp, kreal, grid, batch, weight, wpb, scratch, scratch_bytes, st);
+        if (rc != DMR_ERR_UNSUPPORTED) return rc;
+    }
     const int cw = cube_width(p->g);
     if (cw > 0 && (det || (p->g.ndim == 3 && grid_variant() == 1))) {
         switch (p->g.ndim * 100 + cw) {
@@ -1421,5 +1416,5 @@ extern "C" int dmr_grid(const dmr_plan *p, const void *kspace, int kspace_real, 
     DMR_CHECK(batch >= 0, DMR_ERR_INVALID, "negative batch");
     if (batch == 0) return DMR_OK;
     return grid_dispatch(p, kspace, kspace_real, (float2 *)grid, batch, weight, weight_per_batch,
-                         deterministic, (cudaStream_t)stream);
+                         deterministic, nullptr, 0, (cudaStream_t)stream);
 }

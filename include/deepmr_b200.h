@@ -126,8 +126,13 @@ int dmr_interp(const dmr_plan *plan, const void *grid, void *kspace,
  *  grid: (batch, nframes, *os_shape) complex64, fully written.
  *  deterministic: 0 = shared-memory tiles flushed with global atomics
  *     (summation order may vary between runs);
- *     1 = each tile is owned by one warp which sums its contributions in a
- *     fixed order (bitwise reproducible, no atomics).
+ *     1 = every grid point is summed by one owner in a fixed order (bitwise
+ *     reproducible, no float atomics): 3D grids of 8 or more coils keep
+ *     8^3-point block regions in registers (regions too dense for one block
+ *     are split into partial sums added in a fixed order; without a caller
+ *     workspace this call takes their scratch from a library-owned
+ *     stream-ordered memory pool); other grids run the bins in colour passes
+ *     of disjoint tiles.
  */
 int dmr_grid(const dmr_plan *plan, const void *kspace, int kspace_real,
              void *grid, int64_t batch, const float *weight,
