@@ -321,6 +321,10 @@ def run_b200(args):
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "alg_bytes_per_launch": kbytes}
 
+    serving = None
+    if not args.no_extras and rank == 0:
+        serving = run_serving(dev)
+
     # end to end through the public API: pinned host buffers, copies in the timed region
     e2e = None
     if not args.no_e2e:
@@ -371,13 +375,42 @@ def run_b200(args):
                        if not args.small else "inputs larger than L2",
                        "parallelism": f"replicas x{world} (one independent workload per GPU)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "extras": extras,
+            "clocks": ck, "extras": extras, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# serving: CG-SENSE requests, continuous batching vs the plain per-call path
+# ---------------------------------------------------------------------------
+def run_serving(dev, nreq=32, seed=0):
+    """CG-SENSE serving workload (20 CG iterations, Toeplitz; matrix uniform over
+    {128, 192, 256, 320}^2, coils over {8, 16, 32}, radial or spiral): all
+    requests at once (burst), then Poisson arrivals at 80% of the plain path's
+    burst throughput. Latency = arrival to result on the host."""
+    from deepmr_b200 import recon
+
+    burst = recon.synthetic_requests(nreq, rate_hz=1e6, seed=seed)
+    srv = recon.ReconServer(device=dev, max_active=8, hbm_budget=32 << 30)
+    srv.prepare(burst)
+    srv.run(burst[:4], realtime=False)  # warm the allocator and the graphs
+    srv.run_sequential(burst[:4], realtime=False)
+    out = {"workload": f"{nreq} CG-SENSE requests, 20 iterations, Toeplitz normal operator, "
+                       "matrix {128,192,256,320}^2, coils {8,16,32}, radial or spiral"}
+    seq = srv.run_sequential(burst, realtime=False).summary()
+    cont = srv.run(burst, realtime=False).summary()
+    out["burst"] = {"plain": seq, "continuous": cont}
+    rate = 0.8 * seq["throughput_rps"]
+    pois = recon.synthetic_requests(nreq, rate_hz=rate, seed=seed + 1)
+    srv.prepare(pois)
+    out["poisson"] = {"rate_hz": rate, "plain": srv.run_sequential(pois).summary(),
+                      "continuous": srv.run(pois).summary()}
+    torch.cuda.synchronize(dev)
+    return out
 
 
 # ---------------------------------------------------------------------------

@@ -14,13 +14,16 @@ Here:
 * `ReconServer` admits requests of different matrix sizes, coil counts and
   trajectories as device memory (an HBM budget) and request slots free up,
   keeps plans, Toeplitz kernels and coil maps resident across requests, and
-  advances every admitted request by one CG iteration per round, each on its
-  own CUDA stream, so their work overlaps on the GPU (continuous batching at
-  iteration granularity). `run_sequential` is the plain per-call path: one
-  request at a time, to completion.
+  enqueues every admitted request's whole solve on its own CUDA stream, so up
+  to `max_active` solves overlap on the GPU (continuous batching: requests
+  that arrive while others run are admitted as slots and memory free up).
+  Each request runs in a resident slot whose CG iteration is a captured CUDA
+  graph (one launch per iteration). `run_sequential` is the plain per-call
+  path: one request at a time, to completion, with eager launches.
 
-Every reduction has a fixed order, so a request's result does not depend on
-what else runs beside it (bitwise).
+The CG reductions have a fixed order; with deterministic AHy gridding a
+request's result does not depend on what else runs beside it (bitwise), with
+atomic gridding (the server's default, faster) it agrees to float32 rounding.
 """
 
 import ctypes
@@ -117,13 +120,14 @@ class CGState:
         return v.value
 
 
-def sense_adjoint(kspace, plan, maps, dcf=None):
+def sense_adjoint(kspace, plan, maps, dcf=None, deterministic=True):
     """AHy = sum_c conj(S_c) nufft_adj(dcf * y_c) (E^H(dcf**0.5 y), classic_recon.py:153-156).
 
-    Gridding runs in the deterministic mode, so AHy (and the whole
-    reconstruction) is bitwise independent of concurrent work.
+    With deterministic gridding AHy (and the whole reconstruction) is bitwise
+    independent of concurrent work; atomic gridding is faster and agrees to
+    float32 rounding.
     """
-    img = _nufft._apply_nufft_adj(kspace, plan, None, dcf, None, 128, deterministic=True)
+    img = _nufft._apply_nufft_adj(kspace, plan, None, dcf, None, 128, deterministic=deterministic)
     return (maps.conj() * img).sum(0)
 
 
@@ -170,14 +174,52 @@ class ReconRequest:
     arrival: float = 0.0  # seconds after the start of the run
 
 
+class _Slot:
+    """Resident CG working set of one request at a time, with its stream and a
+    CUDA graph of one CG iteration (normal operator + update) captured on it:
+    an iteration is one graph launch instead of a dozen kernel launches."""
+
+    def __init__(self, normal, dev, use_graph=True):
+        self.stream = torch.cuda.Stream(dev)
+        ishape = tuple(normal.ishape)
+        with torch.cuda.stream(self.stream):
+            self.cg = CGState(torch.zeros(ishape, dtype=torch.complex64, device=dev), normal)
+            # one eager iteration: cuFFT plans and every lazy setup exist before capture
+            self.cg.init(self.stream)
+            self.cg.step(self.stream)
+        self.stream.synchronize()
+        self.graph = None
+        if use_graph:
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph, stream=self.stream):
+                self.cg.step(self.stream)
+            self.stream.synchronize()
+        self.cg.steps = 0
+
+    def start(self, ahy):
+        """Load a request's AHy (on the slot's stream) and initialise CG."""
+        self.cg.ahy.copy_(ahy)
+        self.cg.init(self.stream)
+        self.cg.steps = 0
+
+    def step(self):
+        if self.graph is not None:
+            with torch.cuda.stream(self.stream):
+                self.graph.replay()
+            self.cg.steps += 1
+        else:
+            with torch.cuda.stream(self.stream):
+                self.cg.step(self.stream)
+
+
 @dataclass
 class _Active:
     req: ReconRequest
-    stream: torch.cuda.Stream
-    cg: CGState
+    slot: _Slot
     nbytes: int
     done_event: object = None
     started: float = 0.0
+    result: object = None
 
 
 @dataclass
@@ -203,16 +245,22 @@ class ReconServer:
     hbm_budget: bytes of device memory the active requests' working sets may
     use (resident plans/kernels/maps are accounted separately, in the caches).
     max_active: request slots.
+    deterministic: grid AHy deterministically (results bitwise independent of
+    the mix); otherwise with atomics (results agree to float32 rounding).
     """
 
-    def __init__(self, device="cuda", hbm_budget=16 << 30, max_active=8, width=4, gram_width=6):
+    def __init__(self, device="cuda", hbm_budget=16 << 30, max_active=8, width=4, gram_width=6,
+                 use_graphs=True, deterministic=False):
         self.dev = _nufft.compute_device(device)
         self.budget = int(hbm_budget)
         self.max_active = int(max_active)
         self.width, self.gram_width = width, gram_width
+        self.use_graphs = bool(use_graphs)
+        self.deterministic = bool(deterministic)
         self.plans = {}  # traj_key -> (plan, gram, dcf tensor)
         self.maps = {}  # maps_key -> tensor
         self.normals = {}  # (traj_key, maps_key, lamda) -> SenseNormal
+        self.slots = {}  # normal key -> free _Slot list (resident working sets + graphs)
 
     # resident caches --------------------------------------------------------
     def _plan(self, req):
@@ -243,59 +291,81 @@ class ReconServer:
         return 8 * (6 * isize + 2 * ncoils * G + ncoils * isize + ncoils * K) + (1 << 20) * ndim
 
     def prepare(self, requests):
-        """Build the resident plans, Toeplitz kernels, coil maps (and cuFFT plans)."""
+        """Build the resident plans, Toeplitz kernels, coil maps (and cuFFT
+        plans), and the CG slots (with their captured iteration) the requests
+        can use at once."""
+        need = {}
         for r in requests:
             self._plan(r)
-            self._normal(r)
+            key = self._key(r)
+            need[key] = min(need.get(key, 0) + 1, self.max_active)
+            free = self.slots.setdefault(key, [])
+            while len(free) < need[key]:
+                free.append(_Slot(self._normal(r), self.dev, self.use_graphs))
+
+    @staticmethod
+    def _key(req):
+        return (req.traj_key, req.maps_key, float(req.lamda))
+
+    def _take_slot(self, req):
+        free = self.slots.setdefault(self._key(req), [])
+        return free.pop() if free else _Slot(self._normal(req), self.dev, self.use_graphs)
 
     def _start(self, req, now):
-        s = torch.cuda.Stream(self.dev)
-        with torch.cuda.stream(s):
+        slot = self._take_slot(req)
+        with torch.cuda.stream(slot.stream):
             plan, gram, dcf = self._plan(req)
             normal = self._normal(req)
             y = torch.as_tensor(req.kspace).to(self.dev, torch.complex64, non_blocking=True)
-            ahy = sense_adjoint(y, plan, normal.maps, dcf)
-            cg = CGState(ahy, normal)
-            cg.init(s)
-        return _Active(req, s, cg, self.request_bytes(req), started=now)
+            slot.start(sense_adjoint(y, plan, normal.maps, dcf, self.deterministic))
+        return _Active(req, slot, self.request_bytes(req), started=now)
 
     def run(self, requests, realtime=True):
-        """Serve `requests` (their `arrival` times are honoured when realtime)."""
+        """Serve `requests` (their `arrival` times are honoured when realtime).
+
+        A request is admitted when it has arrived, a slot is free and its
+        working set fits the HBM budget; admission enqueues its whole solve
+        (AHy, CG init, one graph launch per iteration) on its slot's stream,
+        so up to `max_active` solves run concurrently on the GPU while the
+        host only admits and retires."""
         stats = ServeStats()
         pending = sorted(requests, key=lambda r: r.arrival)
         active, used = [], 0
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
-            # admission: arrived, a free slot, and room in the HBM budget
+            # admission: arrived, a free slot, and room in the HBM budget (FIFO)
             while pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active:
                 nb = self.request_bytes(pending[0])
                 if active and used + nb > self.budget:
                     break
                 req = pending.pop(0)
-                active.append(self._start(req, now))
+                a = self._start(req, now)
+                for _ in range(req.niter):
+                    a.slot.step()
+                with torch.cuda.stream(a.slot.stream):
+                    a.result = a.slot.cg.x.clone()  # the slot is reused: the result leaves it
+                a.done_event = torch.cuda.Event()
+                a.done_event.record(a.slot.stream)
+                active.append(a)
                 used += nb
             stats.peak_active = max(stats.peak_active, len(active))
-            if not active:
-                time.sleep(max(0.0, min(pending[0].arrival - now, 0.002)))
-                continue
-            # one CG iteration per active request, each on its own stream
-            for a in active:
-                if a.cg.steps < a.req.niter:
-                    with torch.cuda.stream(a.stream):
-                        a.cg.step(a.stream)
-                    if a.cg.steps == a.req.niter:
-                        a.done_event = torch.cuda.Event()
-                        a.done_event.record(a.stream)
             # retire finished requests
             still = []
             for a in active:
-                if a.done_event is not None and a.done_event.query():
+                if a.done_event.query():
                     stats.latency[a.req.rid] = time.perf_counter() - t0 - a.req.arrival
-                    stats.results[a.req.rid] = a.cg.x
+                    stats.results[a.req.rid] = a.result
+                    self.slots[self._key(a.req)].append(a.slot)
                     used -= a.nbytes
                 else:
                     still.append(a)
+            if len(still) == len(active):
+                # nothing finished: wait a little (for a completion or the next arrival)
+                wait = 5e-5
+                if pending and not active:
+                    wait = max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 2e-3))
+                time.sleep(wait)
             active = still
         torch.cuda.synchronize(self.dev)
         stats.wall = time.perf_counter() - t0
@@ -312,7 +382,7 @@ class ReconServer:
             plan, gram, dcf = self._plan(req)
             normal = self._normal(req)
             y = torch.as_tensor(req.kspace).to(self.dev, torch.complex64)
-            cg = CGState(sense_adjoint(y, plan, normal.maps, dcf), normal)
+            cg = CGState(sense_adjoint(y, plan, normal.maps, dcf, self.deterministic), normal)
             cg.init()
             for _ in range(req.niter):
                 cg.step()

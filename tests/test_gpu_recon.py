@@ -70,17 +70,34 @@ def test_serving_results_identical_alone_and_in_mix():
     from deepmr_b200 import recon
 
     reqs = _requests()
-    server = recon.ReconServer(device="cuda", max_active=6)
+    server = recon.ReconServer(device="cuda", max_active=6, deterministic=True)
     server.prepare(reqs)
     mixed = server.run(reqs, realtime=False)
     assert mixed.peak_active > 1  # the work really overlapped
     alone = server.run_sequential(reqs, realtime=False)
-    one_slot = recon.ReconServer(device="cuda", max_active=1)
+    one_slot = recon.ReconServer(device="cuda", max_active=1, deterministic=True)
     one_slot.prepare(reqs)
     single = one_slot.run(reqs, realtime=False)
     for r in reqs:
         assert torch.equal(mixed.results[r.rid], alone.results[r.rid]), r.rid
         assert torch.equal(single.results[r.rid], alone.results[r.rid]), r.rid
+
+
+def test_serving_atomic_gridding_same_alone_and_in_mix_within_tolerance():
+    """The default server grids AHy with atomics: results agree to float32 rounding."""
+    from deepmr_b200 import recon
+
+    reqs = _requests()
+    server = recon.ReconServer(device="cuda", max_active=6)
+    server.prepare(reqs)
+    mixed = server.run(reqs, realtime=False)
+    alone = server.run_sequential(reqs, realtime=False)
+    det = recon.ReconServer(device="cuda", max_active=6, deterministic=True)
+    det.prepare(reqs)
+    ref = det.run_sequential(reqs, realtime=False)
+    for r in reqs:
+        assert rel(mixed.results[r.rid], alone.results[r.rid]) < 1e-5, r.rid
+        assert rel(mixed.results[r.rid], ref.results[r.rid]) < 1e-5, r.rid
 
 
 def test_serving_admission_respects_budget():
