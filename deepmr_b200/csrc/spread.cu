@@ -1139,15 +1139,24 @@ static Region cube_region(const Geom &g, int CC)
     return r;
 }
 
-// coils per block: power of two covering the batch, at most 32 / NG, reduced
-// until the tile + staged samples fit in shared memory
+// coils per block: power of two covering the batch, at most 32 / NG and
+// max_coils, reduced until the tile + staged samples fit in shared memory.
+// 3D interpolation caps at 16 coils (smaller tiles, more resident blocks:
+// 15.6 vs 17.4 ms on the 192^3 kooshball with 32 coils); gridding keeps 32 (its
+// per-sample weights are shared by more coils: 34.1 vs 35.2 ms).
 template <int NDIM, int W>
-static int cube_config(const Geom &g, int64_t batch, Region &rg, size_t &smem)
+static int cube_config(const Geom &g, int64_t batch, Region &rg, size_t &smem, int max_coils)
 {
     using S = CubeShape<NDIM, W>;
     const size_t limit = (size_t)max_smem();
+    // DMR_CUBE_MAX_COILS overrides the cap on coils per block (tuning)
+    static const int env_cap = [] {
+        const char *e = getenv("DMR_CUBE_MAX_COILS");
+        return e ? std::max(1, atoi(e)) : 0;
+    }();
+    const int cap = env_cap ? env_cap : max_coils;
     int l = 0;
-    while ((1ll << l) < batch && (1 << l) * S::NG < 32) l++;
+    while ((1ll << l) < batch && (1 << l) * S::NG < 32 && (2 << l) <= cap) l++;
     for (; l >= 0; l--) {
         rg = cube_region<NDIM, W>(g, 1 << l);
         smem = S::meta_bytes() + (size_t)(1 << l) * rg.PP * sizeof(float2);
@@ -1162,7 +1171,7 @@ static int launch_interp_cube(const dmr_plan *p, const float2 *grid, float2 *ksp
 {
     Region rg;
     size_t smem = 0;
-    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem);
+    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem, NDIM == 3 ? 16 : 32);
     DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "interpolation tile does not fit in shared memory");
     auto kern = interp_cube_kernel<NDIM, W>;
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1181,7 +1190,7 @@ static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float
 {
     Region rg;
     size_t smem = 0;
-    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem);
+    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem, 32);
     DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "gridding tile does not fit in shared memory");
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->nwork == 0) return DMR_OK;
