@@ -387,26 +387,30 @@ def run_b200(args):
 # ---------------------------------------------------------------------------
 # serving: CG-SENSE requests, continuous batching vs the plain per-call path
 # ---------------------------------------------------------------------------
-def run_serving(dev, nreq=32, seed=0):
+def run_serving(dev, nreq=64, seed=0, max_active=4):
     """CG-SENSE serving workload (20 CG iterations, Toeplitz; matrix uniform over
     {128, 192, 256, 320}^2, coils over {8, 16, 32}, radial or spiral): all
     requests at once (burst), then Poisson arrivals at 80% of the plain path's
-    burst throughput. Latency = arrival to result on the host."""
+    burst throughput. Both paths run every request set once untimed first
+    (plans, caching allocator, graphs). Latency = arrival to result on the host."""
     from deepmr_b200 import recon
 
     burst = recon.synthetic_requests(nreq, rate_hz=1e6, seed=seed)
-    srv = recon.ReconServer(device=dev, max_active=8, hbm_budget=32 << 30)
+    srv = recon.ReconServer(device=dev, max_active=max_active, hbm_budget=32 << 30)
     srv.prepare(burst)
-    srv.run(burst[:4], realtime=False)  # warm the allocator and the graphs
-    srv.run_sequential(burst[:4], realtime=False)
+    srv.run(burst, realtime=False)
+    srv.run_sequential(burst, realtime=False)
     out = {"workload": f"{nreq} CG-SENSE requests, 20 iterations, Toeplitz normal operator, "
-                       "matrix {128,192,256,320}^2, coils {8,16,32}, radial or spiral"}
+                       "matrix {128,192,256,320}^2, coils {8,16,32}, radial or spiral",
+           "max_active": max_active}
     seq = srv.run_sequential(burst, realtime=False).summary()
     cont = srv.run(burst, realtime=False).summary()
     out["burst"] = {"plain": seq, "continuous": cont}
     rate = 0.8 * seq["throughput_rps"]
     pois = recon.synthetic_requests(nreq, rate_hz=rate, seed=seed + 1)
     srv.prepare(pois)
+    srv.run(pois, realtime=False)
+    srv.run_sequential(pois, realtime=False)
     out["poisson"] = {"rate_hz": rate, "plain": srv.run_sequential(pois).summary(),
                       "continuous": srv.run(pois).summary()}
     torch.cuda.synchronize(dev)
