@@ -505,6 +505,7 @@ __device__ __forceinline__ LaneMap lane_map(int cc_log2)
 }
 
 constexpr int kCubeThreads = 128;
+constexpr int kPf = 4;  // samples whose k-space values a gridding lane loads ahead
 
 template <int NDIM, int W>
 __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
@@ -649,15 +650,35 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
                     }
                 }
         };
+        // the k-space values (and density weights) of the next kPf samples are
+        // loaded ahead: a warp otherwise waits a full global-load latency per sample
+        float2 pv[kPf];
+        float pw[kPf];
+        auto fetch = [&](int q, float2 &v, float &wt) {
+            v = make_float2(0.0f, 0.0f);
+            wt = 1.0f;
+            if (q < q1) {
+                const int64_t o2 = b * g.total + gi[q];
+                v = load_sample(ksp, kreal, o2);
+                if (weight) wt = weight[wpb ? o2 : (int64_t)gi[q]];
+            }
+        };
+#pragma unroll
+        for (int k = 0; k < kPf; k++) fetch(q0 + k, pv[k], pw[k]);
         for (int q = q0; q < q1; q++) {
             const int o = off[q];
             if (o != cur) {
                 if (cur >= 0) flush(cur);
                 cur = o;
             }
-            const int64_t o2 = b * g.total + gi[q];
-            float2 v = load_sample(ksp, kreal, o2);
-            if (weight) v = __fmul2_rn(v, f2(weight[wpb ? o2 : (int64_t)gi[q]]));
+            float2 v = pv[0];
+            if (weight) v = __fmul2_rn(v, f2(pw[0]));
+#pragma unroll
+            for (int k = 0; k + 1 < kPf; k++) {
+                pv[k] = pv[k + 1];
+                pw[k] = pw[k + 1];
+            }
+            fetch(q + kPf, pv[kPf - 1], pw[kPf - 1]);
             const float *w = wts + q * NW;
 #pragma unroll
             for (int sl = 0; sl < SPL; sl++) {
