@@ -341,10 +341,10 @@ __global__ void __launch_bounds__(256) grid_atomic_kernel(
 // streams per warp. Complex arithmetic uses the packed FP32 instructions
 // (__ffma2_rn / __fmul2_rn).
 // ---------------------------------------------------------------------------
-template <int NDIM, int W>
+template <int NDIM, int W, int CR = 64>
 struct CubeShape {
     static constexpr int INS = NDIM == 3 ? W * W : (NDIM == 2 ? W : 1);  // taps per slice
-    static constexpr int SPL0 = 64 / INS;                                 // slices that fit in 64 regs
+    static constexpr int SPL0 = CR / INS;                                 // slices that fit in CR complex regs
     static constexpr int SPL = SPL0 >= W ? W : (SPL0 < 1 ? 1 : SPL0);     // slices per lane
     static constexpr int NGR = (W + SPL - 1) / SPL;                       // groups needed
     static constexpr int NG = NGR <= 1 ? 1 : (NGR <= 2 ? 2 : (NGR <= 4 ? 4 : (NGR <= 8 ? 8 : 16)));
@@ -595,14 +595,14 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     }
 }
 
-template <int NDIM, int W>
+template <int NDIM, int W, int CR>
 __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
     Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
     const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
     const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid, int64_t batch,
     const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
 {
-    using S = CubeShape<NDIM, W>;
+    using S = CubeShape<NDIM, W, CR>;
     constexpr int NG = S::NG, SPL = S::SPL, INS = S::INS, NW = S::NW;
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
@@ -1127,10 +1127,10 @@ static int pad_mod16(int x, int m)
     return x + (((m - x) % 16) + 16) % 16;
 }
 
-template <int NDIM, int W>
+template <int NDIM, int W, int CR = 64>
 static Region cube_region(const Geom &g, int CC)
 {
-    using S = CubeShape<NDIM, W>;
+    using S = CubeShape<NDIM, W, CR>;
     Region r;
     r.R0 = g.T[0] + W - 1;
     r.R1 = NDIM > 1 ? g.T[1] + W - 1 : 1;
@@ -1165,10 +1165,10 @@ static Region cube_region(const Geom &g, int CC)
 // 3D interpolation caps at 16 coils (smaller tiles, more resident blocks:
 // 15.6 vs 17.4 ms on the 192^3 kooshball with 32 coils); gridding keeps 32 (its
 // per-sample weights are shared by more coils: 34.1 vs 35.2 ms).
-template <int NDIM, int W>
+template <int NDIM, int W, int CR = 64>
 static int cube_config(const Geom &g, int64_t batch, Region &rg, size_t &smem, int max_coils)
 {
-    using S = CubeShape<NDIM, W>;
+    using S = CubeShape<NDIM, W, CR>;
     const size_t limit = (size_t)max_smem();
     // DMR_CUBE_MAX_COILS overrides the cap on coils per block (tuning)
     static const int env_cap = [] {
@@ -1179,7 +1179,7 @@ static int cube_config(const Geom &g, int64_t batch, Region &rg, size_t &smem, i
     int l = 0;
     while ((1ll << l) < batch && (1 << l) * S::NG < 32 && (2 << l) <= cap) l++;
     for (; l >= 0; l--) {
-        rg = cube_region<NDIM, W>(g, 1 << l);
+        rg = cube_region<NDIM, W, CR>(g, 1 << l);
         smem = S::meta_bytes() + (size_t)(1 << l) * rg.PP * sizeof(float2);
         if (smem <= limit) return l;
     }
@@ -1211,11 +1211,15 @@ static int launch_grid_cube(const dmr_plan *p, const void *ksp, int kreal, float
 {
     Region rg;
     size_t smem = 0;
-    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem, 32);
+    // 3D: one 16-tap slice per lane (4 lanes per coil, 8 coils per warp): 27.1
+    // vs 32.9 ms with the whole 64-tap cube per lane on the 192^3 kooshball
+    // (fewer registers, more resident warps)
+    constexpr int CR = NDIM == 3 ? 16 : 64;
+    const int l = cube_config<NDIM, W, CR>(p->g, batch, rg, smem, 32);
     DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "gridding tile does not fit in shared memory");
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->nwork == 0) return DMR_OK;
-    auto kern = grid_cube_kernel<NDIM, W>;
+    auto kern = grid_cube_kernel<NDIM, W, CR>;
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t chunks = ceil_div(batch, 1ll << l);
     DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
