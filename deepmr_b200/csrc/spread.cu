@@ -637,15 +637,20 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
         for (int sl = 0; sl < SPL; sl++)
 #pragma unroll
             for (int j = 0; j < INS; j++) cube[sl][j] = make_float2(0.0f, 0.0f);
+        const int flip = (threadIdx.x >> 4) & 1;
         auto flush = [&](int o) {
 #pragma unroll
             for (int sl = 0; sl < SPL; sl++)
                 if (z0 + sl < W) {
 #pragma unroll
                     for (int j = 0; j < INS; j++) {
-                        float2 *p = ctile + o + sl * rg.SP + inner_off<NDIM, W>(j, rg.R0);
-                        atomicAdd(&p->x, cube[sl][j].x);
-                        atomicAdd(&p->y, cube[sl][j].y);
+                        // the upper half-warp adds the imaginary part first: the two
+                        // halves then hit odd and even words, all 32 banks
+                        float *p = reinterpret_cast<float *>(ctile + o + sl * rg.SP + inner_off<NDIM, W>(j, rg.R0));
+                        const float a = flip ? cube[sl][j].y : cube[sl][j].x;
+                        const float c = flip ? cube[sl][j].x : cube[sl][j].y;
+                        atomicAdd(p + flip, a);
+                        atomicAdd(p + 1 - flip, c);
                         cube[sl][j] = make_float2(0.0f, 0.0f);
                     }
                 }
