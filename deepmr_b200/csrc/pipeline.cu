@@ -43,48 +43,52 @@ struct ResizeArgs {
     int in_real;
 };
 
-__global__ void resize_kernel(ResizeArgs r, const void *__restrict__ in, float2 *__restrict__ out)
+__global__ void __launch_bounds__(128) resize_kernel(ResizeArgs r, const void *__restrict__ in,
+                                                     float2 *__restrict__ out)
 {
-    for (int64_t bi = blockIdx.y; bi < r.nbatch; bi += gridDim.y) {
-        const int64_t ibase = bi * r.isize;
-        const int64_t obase = bi * r.osize;
-        for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < r.osize;
-             q += (int64_t)gridDim.x * blockDim.x) {
-            const int qx = (int)(q % r.O[0]);
-            const int64_t t = q / r.O[0];
-            const int qy = (int)(t % r.O[1]);
-            const int qz = (int)(t / r.O[1]);
-            const int qq[3] = {qx, qy, qz};
-            bool valid = true;
-            int li[3], lo[3], pi[3];
+    // one output row (fixed y, z, batch) per block step: the row's y/z index
+    // arithmetic and apodisation are computed once, threads run along x
+    const int64_t rows_per_batch = (int64_t)r.O[1] * r.O[2];
+    const int64_t nrows = rows_per_batch * r.nbatch;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+        const int64_t bi = row / rows_per_batch;
+        const int rr = (int)(row - bi * rows_per_batch);
+        const int qq[3] = {0, rr % r.O[1], rr / r.O[1]};
+        bool rvalid = true;
+        int li[3], lo[3], pi[3];
+        float rs = r.scale;
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-                lo[a] = qq[a] + r.oroll[a];
-                if (lo[a] >= r.O[a]) lo[a] -= r.O[a];
-                valid = valid && lo[a] >= r.so[a] && lo[a] < r.so[a] + r.cp[a];
-                li[a] = lo[a] - r.so[a] + r.si[a];
-                pi[a] = li[a] + r.iroll[a];
-                if (pi[a] >= r.I[a]) pi[a] -= r.I[a];
-            }
+        for (int a = 1; a < 3; a++) {
+            lo[a] = qq[a] + r.oroll[a];
+            if (lo[a] >= r.O[a]) lo[a] -= r.O[a];
+            rvalid = rvalid && lo[a] >= r.so[a] && lo[a] < r.so[a] + r.cp[a];
+            li[a] = lo[a] - r.so[a] + r.si[a];
+            pi[a] = li[a] + r.iroll[a];
+            if (pi[a] >= r.I[a]) pi[a] -= r.I[a];
+            if (rvalid && r.apod[a]) rs *= r.apod[a][r.apod_on_output ? lo[a] : li[a]];
+        }
+        float2 *orow = out + bi * r.osize + (int64_t)rr * r.O[0];
+        if (!rvalid) {
+            for (int qx = threadIdx.x; qx < r.O[0]; qx += blockDim.x) orow[qx] = make_float2(0.0f, 0.0f);
+            continue;
+        }
+        const int64_t irow = bi * r.isize + ((int64_t)pi[2] * r.I[1] + pi[1]) * r.I[0];
+        for (int qx = threadIdx.x; qx < r.O[0]; qx += blockDim.x) {
+            int lx = qx + r.oroll[0];
+            if (lx >= r.O[0]) lx -= r.O[0];
             float2 v = make_float2(0.0f, 0.0f);
-            if (valid) {
-                const int64_t ii = ibase + ((int64_t)pi[2] * r.I[1] + pi[1]) * r.I[0] + pi[0];
-                if (r.in_real) v.x = reinterpret_cast<const float *>(in)[ii];
-                else v = reinterpret_cast<const float2 *>(in)[ii];
-                if (r.scale != 1.0f) {
-                    v.x *= r.scale;
-                    v.y *= r.scale;
-                }
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    if (r.apod[a]) {
-                        const float ap = r.apod[a][r.apod_on_output ? lo[a] : li[a]];
-                        v.x *= ap;
-                        v.y *= ap;
-                    }
-                }
+            if (lx >= r.so[0] && lx < r.so[0] + r.cp[0]) {
+                const int ix = lx - r.so[0] + r.si[0];
+                int px = ix + r.iroll[0];
+                if (px >= r.I[0]) px -= r.I[0];
+                if (r.in_real) v.x = reinterpret_cast<const float *>(in)[irow + px];
+                else v = reinterpret_cast<const float2 *>(in)[irow + px];
+                float sc = rs;
+                if (r.apod[0]) sc *= r.apod[0][r.apod_on_output ? lx : ix];
+                v.x *= sc;
+                v.y *= sc;
             }
-            out[obase + q] = v;
+            orow[qx] = v;
         }
     }
 }
@@ -103,12 +107,9 @@ static int launch_resize(const ResizeArgs &r, const void *in, float2 *out, cudaS
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int threads = 256;
-    const int64_t want = ceil_div(r.osize, threads);
-    const int64_t gy = std::min<int64_t>(r.nbatch, 65535);
-    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8 / std::max<int64_t>(1, std::min<int64_t>(gy, 8)) + 1));
-    dim3 grd((unsigned)std::min<int64_t>(gx, want), (unsigned)gy);
-    resize_kernel<<<grd, threads, 0, st>>>(r, in, out);
+    const int64_t nrows = (int64_t)r.O[1] * r.O[2] * r.nbatch;
+    const unsigned blocks = (unsigned)std::min<int64_t>(nrows, (int64_t)sms * 64);
+    resize_kernel<<<blocks, 128, 0, st>>>(r, in, out);
     DMR_LAUNCHED("resize_kernel");
     return DMR_OK;
 }
