@@ -506,15 +506,16 @@ __device__ __forceinline__ LaneMap lane_map(int cc_log2)
 
 constexpr int kCubeThreads = 128;
 constexpr int kPf = 4;  // samples whose k-space values a gridding lane loads ahead
+constexpr int kInterpCubeRegs = 64;  // complex registers of an interpolation lane's cube
 
-template <int NDIM, int W>
+template <int NDIM, int W, int CR>
 __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     Geom g, Region rg, const WorkItem *__restrict__ work, const float *__restrict__ sc0,
     const float *__restrict__ sc1, const float *__restrict__ sc2, const int32_t *__restrict__ sidx,
     const float2 *__restrict__ grid, float2 *__restrict__ ksp, int64_t batch,
     const float *__restrict__ weight, int wpb, float inv_scale, int cc_log2)
 {
-    using S = CubeShape<NDIM, W>;
+    using S = CubeShape<NDIM, W, CR>;
     constexpr int NG = S::NG, SPL = S::SPL, INS = S::INS, NW = S::NW;
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
@@ -1197,9 +1198,10 @@ static int launch_interp_cube(const dmr_plan *p, const float2 *grid, float2 *ksp
 {
     Region rg;
     size_t smem = 0;
-    const int l = cube_config<NDIM, W>(p->g, batch, rg, smem, NDIM == 3 ? 16 : 32);
+    constexpr int CR = kInterpCubeRegs;
+    const int l = cube_config<NDIM, W, CR>(p->g, batch, rg, smem, NDIM == 3 ? 16 : 32);
     DMR_CHECK(l >= 0, DMR_ERR_UNSUPPORTED, "interpolation tile does not fit in shared memory");
-    auto kern = interp_cube_kernel<NDIM, W>;
+    auto kern = interp_cube_kernel<NDIM, W, CR>;
     DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t chunks = ceil_div(batch, 1ll << l);
     DMR_CHECK(chunks < 65536, DMR_ERR_UNSUPPORTED, "batch too large");
