@@ -203,21 +203,38 @@ static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, Nufft
     return DMR_OK;
 }
 
-__global__ void cmul_kernel(float2 *__restrict__ data, const float2 *__restrict__ kern, int64_t ksize,
-                            int64_t nk, int64_t nbatch, float s)
+__device__ __forceinline__ float2 cmul_scaled(float2 k, float2 d, float s)
 {
-    const int64_t n = ksize * nbatch;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t bi = e / ksize;
-        const int64_t q = e - bi * ksize;
-        const float2 k = kern[(bi % nk) * ksize + q];
-        const float2 d = data[e];
-        // kernel value times spectrum (toeplitz.py:86), then the two orthonormal 1/sqrt(K)
-        float2 o = make_float2(k.x * d.x - k.y * d.y, k.x * d.y + k.y * d.x);
-        o.x *= s;
-        o.y *= s;
-        data[e] = o;
+    // kernel value times spectrum (toeplitz.py:86), then the two orthonormal 1/sqrt(K)
+    float2 o = make_float2(k.x * d.x - k.y * d.y, k.x * d.y + k.y * d.x);
+    o.x *= s;
+    o.y *= s;
+    return o;
+}
+
+// data[b] *= kern[b mod nk] * s, per batch row (blockIdx.y); two complex values
+// per thread with 16-byte accesses when vec (even row length, 16-byte aligned
+// data and kernel)
+__global__ void __launch_bounds__(256) cmul_kernel(float2 *__restrict__ data, const float2 *__restrict__ kern,
+                                                   int64_t ksize, int64_t nk, int64_t nbatch, float s, int vec)
+{
+    for (int64_t bi = blockIdx.y; bi < nbatch; bi += gridDim.y) {
+        float2 *d = data + bi * ksize;
+        const float2 *k = kern + (bi % nk) * ksize;
+        const int64_t step = (int64_t)gridDim.x * blockDim.x;
+        if (vec) {
+            float4 *d4 = reinterpret_cast<float4 *>(d);
+            const float4 *k4 = reinterpret_cast<const float4 *>(k);
+            for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ksize / 2; e += step) {
+                const float4 dv = d4[e], kv = __ldg(k4 + e);
+                const float2 a = cmul_scaled(make_float2(kv.x, kv.y), make_float2(dv.x, dv.y), s);
+                const float2 c = cmul_scaled(make_float2(kv.z, kv.w), make_float2(dv.z, dv.w), s);
+                d4[e] = make_float4(a.x, a.y, c.x, c.y);
+            }
+        } else {
+            for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ksize; e += step)
+                d[e] = cmul_scaled(k[e], d[e], s);
+        }
     }
 }
 
@@ -512,9 +529,17 @@ extern "C" int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t
     r.in_real = image_real;
     DMR_TRY(launch_resize(r, image, data, st));
     DMR_TRY(fft_exec(*fp, data, CUFFT_FORWARD, work, st));
-    const int64_t n = batch * ksize;
-    cmul_kernel<<<elem_blocks(n), 256, 0, st>>>(data, (const float2 *)kernel, ksize, nk, batch,
-                                                (float)(1.0 / (double)ksize));
+    {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned gy = (unsigned)std::min<int64_t>(batch, 65535);
+        const int64_t per_row = ceil_div(ksize / 2 + 1, 256);
+        const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>(per_row, ceil_div((int64_t)sms * 16, gy)));
+        const int vec = (ksize % 2 == 0) && ((uintptr_t)data % 16 == 0) && ((uintptr_t)kernel % 16 == 0);
+        cmul_kernel<<<dim3(gx, gy), 256, 0, st>>>(data, (const float2 *)kernel, ksize, nk, batch,
+                                                  (float)(1.0 / (double)ksize), vec);
+    }
     DMR_LAUNCHED("cmul_kernel");
     DMR_TRY(fft_exec(*fp, data, CUFFT_INVERSE, work, st));
     ResizeArgs c;
