@@ -40,6 +40,9 @@ SYMBOLS = (
     "dmr_nufft_workspace_bytes",
     "dmr_nufft_forward",
     "dmr_nufft_adjoint",
+    "dmr_nufft_lowrank_workspace_bytes",
+    "dmr_nufft_forward_lowrank",
+    "dmr_nufft_adjoint_lowrank",
     "dmr_nufft_traj_grad",
     "dmr_toeplitz_workspace_bytes",
     "dmr_toeplitz_finalize",
@@ -94,6 +97,15 @@ _SIGS = {
     "dmr_nufft_adjoint": (
         ctypes.c_int,
         [vp, vp, ctypes.c_int, vp, i64, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t, vp],
+    ),
+    "dmr_nufft_lowrank_workspace_bytes": (ctypes.c_int, [vp, i64, i64, szp]),
+    "dmr_nufft_forward_lowrank": (
+        ctypes.c_int,
+        [vp, vp, ctypes.c_int, i64, vp, vp, i64, vp, ctypes.c_int, vp, ctypes.c_size_t, vp],
+    ),
+    "dmr_nufft_adjoint_lowrank": (
+        ctypes.c_int,
+        [vp, vp, ctypes.c_int, i64, vp, vp, i64, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t, vp],
     ),
     "dmr_nufft_traj_grad": (
         ctypes.c_int,

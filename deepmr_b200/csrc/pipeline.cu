@@ -411,6 +411,211 @@ static int toep_dims(int ndim, const int32_t *kshape, int dims[3], int64_t &ksiz
     return DMR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Low-rank subspace NUFFT (reference: _interpolate_lowrank* / _gridding_lowrank*,
+// src/deepmr/fft/_interp/interp.py:230-357 and grid.py:287-417): frame f of
+// the forward transform interpolates sum_c basis_adjoint[f, c] * FFT(coefficient
+// image c); the adjoint grids every frame and projects with basis[c, f]. The
+// subspace projection commutes with apodisation, padding and the FFT, so the
+// pipelines transform the ncoeff coefficient images and combine grids.
+// ---------------------------------------------------------------------------
+namespace dmr {
+
+constexpr int kMaxCoeff = 32;
+
+// out[b, i, p] = sum_j M[i, j] in[b, j, p] with few inputs (nin <= kMaxCoeff):
+// a thread holds the nin input values of one grid point
+__global__ void __launch_bounds__(256) combine_few_in_kernel(const float2 *__restrict__ in, float2 *__restrict__ out,
+                                                            const float2 *__restrict__ M, int nin, int nout,
+                                                            int64_t npts, int64_t nbatch)
+{
+    for (int64_t b = blockIdx.y; b < nbatch; b += gridDim.y) {
+        for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+             p += (int64_t)gridDim.x * blockDim.x) {
+            float2 v[kMaxCoeff];
+#pragma unroll
+            for (int j = 0; j < kMaxCoeff; j++)
+                v[j] = j < nin ? in[(b * nin + j) * npts + p] : make_float2(0.0f, 0.0f);
+            for (int i = 0; i < nout; i++) {
+                float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+                for (int j = 0; j < kMaxCoeff; j++) {
+                    if (j < nin) {
+                        const float2 m = __ldg(M + (int64_t)i * nin + j);
+                        acc.x += m.x * v[j].x - m.y * v[j].y;
+                        acc.y += m.x * v[j].y + m.y * v[j].x;
+                    }
+                }
+                out[(b * nout + i) * npts + p] = acc;
+            }
+        }
+    }
+}
+
+// the same with few outputs (nout <= kMaxCoeff): a thread streams the inputs
+// of one grid point and keeps the nout sums
+__global__ void __launch_bounds__(256) combine_few_out_kernel(const float2 *__restrict__ in, float2 *__restrict__ out,
+                                                             const float2 *__restrict__ M, int nin, int nout,
+                                                             int64_t npts, int64_t nbatch)
+{
+    for (int64_t b = blockIdx.y; b < nbatch; b += gridDim.y) {
+        for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npts;
+             p += (int64_t)gridDim.x * blockDim.x) {
+            float2 acc[kMaxCoeff];
+#pragma unroll
+            for (int i = 0; i < kMaxCoeff; i++) acc[i] = make_float2(0.0f, 0.0f);
+            for (int j = 0; j < nin; j++) {
+                const float2 v = in[(b * nin + j) * npts + p];
+#pragma unroll
+                for (int i = 0; i < kMaxCoeff; i++) {
+                    if (i < nout) {
+                        const float2 m = __ldg(M + (int64_t)i * nin + j);
+                        acc[i].x += m.x * v.x - m.y * v.y;
+                        acc[i].y += m.x * v.y + m.y * v.x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < kMaxCoeff; i++)
+                if (i < nout) out[(b * nout + i) * npts + p] = acc[i];
+        }
+    }
+}
+
+static int launch_combine(const float2 *in, float2 *out, const float2 *M, int nin, int nout, int64_t npts,
+                          int64_t nbatch, cudaStream_t st)
+{
+    DMR_CHECK(nin <= kMaxCoeff || nout <= kMaxCoeff, DMR_ERR_UNSUPPORTED,
+              "subspace projection with more than %d coefficients", kMaxCoeff);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned gy = (unsigned)std::min<int64_t>(nbatch, 65535);
+    const unsigned gx = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(ceil_div(npts, 256), ceil_div((int64_t)sms * 8, gy)));
+    if (nin <= kMaxCoeff && (nin <= nout || nout > kMaxCoeff))
+        combine_few_in_kernel<<<dim3(gx, gy), 256, 0, st>>>(in, out, M, nin, nout, npts, nbatch);
+    else
+        combine_few_out_kernel<<<dim3(gx, gy), 256, 0, st>>>(in, out, M, nin, nout, npts, nbatch);
+    DMR_LAUNCHED("combine_kernel");
+    return DMR_OK;
+}
+
+struct LowrankWs {
+    float2 *coef;   // (batch, ncoeff, *G)
+    float2 *frame;  // (batch, nframes, *G)
+    void *fft_work;
+    void *rt_scratch;
+    size_t rt_bytes;
+    std::shared_ptr<FftPlan> fft;
+};
+
+static int lowrank_ws(dmr_plan *p, int64_t batch, int64_t ncoeff, void *ws, size_t ws_bytes, LowrankWs &out,
+                      size_t *need)
+{
+    const Geom &g = p->g;
+    DMR_CHECK(ncoeff >= 1 && ncoeff <= kMaxCoeff, DMR_ERR_UNSUPPORTED,
+              "ncoeff must be in [1, %d] (got %lld)", kMaxCoeff, (long long)ncoeff);
+    int dims[3];
+    zyx_dims(g, g.G, dims);
+    int err = DMR_OK;
+    auto fp = get_fft_plan(g.ndim, dims, batch * ncoeff, &err);
+    if (!fp) return err;
+    const size_t coef_bytes = align_up((size_t)batch * ncoeff * g.gsize * sizeof(float2), 256);
+    const size_t frame_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
+    const size_t fft_bytes = align_up(fp->work_bytes, 256);
+    const size_t rt_bytes = align_up(rt_scratch_bytes(p, batch), 256);
+    const size_t total = coef_bytes + frame_bytes + fft_bytes + rt_bytes;
+    if (need) *need = total;
+    if (!ws) return DMR_OK;
+    DMR_CHECK(ws_bytes >= total, DMR_ERR_WORKSPACE, "workspace too small: %zu < %zu", ws_bytes, total);
+    DMR_CHECK(((uintptr_t)ws & 255) == 0, DMR_ERR_INVALID, "workspace must be 256-byte aligned");
+    char *c = (char *)ws;
+    out.coef = (float2 *)c;
+    out.frame = (float2 *)(c + coef_bytes);
+    out.fft_work = fp->work_bytes ? c + coef_bytes + frame_bytes : nullptr;
+    out.rt_scratch = rt_bytes ? c + coef_bytes + frame_bytes + fft_bytes : nullptr;
+    out.rt_bytes = rt_bytes;
+    out.fft = fp;
+    return DMR_OK;
+}
+
+}  // namespace dmr
+
+extern "C" int dmr_nufft_lowrank_workspace_bytes(dmr_plan *p, int64_t batch, int64_t ncoeff, size_t *bytes)
+{
+    DMR_CHECK(p && bytes && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    LowrankWs w;
+    return lowrank_ws(p, batch, ncoeff, nullptr, 0, w, bytes);
+}
+
+extern "C" int dmr_nufft_forward_lowrank(dmr_plan *p, const void *image, int image_real, int64_t ncoeff,
+                                         const void *basis_adjoint, void *kspace, int64_t batch,
+                                         const float *weight, int weight_per_batch, void *workspace,
+                                         size_t workspace_bytes, void *stream)
+{
+    DMR_CHECK(p && image && kspace && basis_adjoint && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geom &g = p->g;
+    LowrankWs w;
+    DMR_TRY(lowrank_ws(p, batch, ncoeff, workspace, workspace_bytes, w, nullptr));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    for (int a = 0; a < 3; a++) {
+        r.O[a] = g.G[a];
+        r.I[a] = g.N[a];
+        r.oroll[a] = g.half[a];  // ifftshift folded in
+        r.iroll[a] = 0;
+        resize_offsets(g.N[a], g.G[a], r.si[a], r.so[a], r.cp[a]);
+        r.apod[a] = (a < g.ndim && g.W[a] != 1) ? p->apod[a] : nullptr;
+    }
+    r.apod_on_output = 0;
+    r.scale = 1.0f;
+    r.nbatch = batch * ncoeff;
+    r.osize = g.gsize;
+    r.isize = g.isize;
+    r.in_real = image_real;
+    DMR_TRY(launch_resize(r, image, w.coef, st));
+    DMR_TRY(fft_exec(*w.fft, w.coef, CUFFT_FORWARD, w.fft_work, st));
+    DMR_TRY(launch_combine(w.coef, w.frame, (const float2 *)basis_adjoint, (int)ncoeff, g.nframes, g.gsize,
+                           batch, st));
+    return interp_dispatch(p, w.frame, (float2 *)kspace, batch, weight, weight_per_batch, st);
+}
+
+extern "C" int dmr_nufft_adjoint_lowrank(dmr_plan *p, const void *kspace, int kspace_real, int64_t ncoeff,
+                                         const void *basis, void *image, int64_t batch, const float *weight,
+                                         int weight_per_batch, int deterministic, void *workspace,
+                                         size_t workspace_bytes, void *stream)
+{
+    DMR_CHECK(p && image && kspace && basis && batch >= 1, DMR_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geom &g = p->g;
+    LowrankWs w;
+    DMR_TRY(lowrank_ws(p, batch, ncoeff, workspace, workspace_bytes, w, nullptr));
+    DMR_TRY(grid_dispatch(p, kspace, kspace_real, w.frame, batch, weight, weight_per_batch, deterministic,
+                          w.rt_scratch, w.rt_bytes, st));
+    DMR_TRY(launch_combine(w.frame, w.coef, (const float2 *)basis, g.nframes, (int)ncoeff, g.gsize, batch, st));
+    DMR_TRY(fft_exec(*w.fft, w.coef, CUFFT_INVERSE, w.fft_work, st));
+    ResizeArgs r;
+    memset(&r, 0, sizeof(r));
+    for (int a = 0; a < 3; a++) {
+        r.O[a] = g.N[a];
+        r.I[a] = g.G[a];
+        r.oroll[a] = 0;
+        r.iroll[a] = g.G[a] - g.half[a];  // fftshift folded in
+        if (r.iroll[a] == g.G[a]) r.iroll[a] = 0;
+        resize_offsets(g.G[a], g.N[a], r.si[a], r.so[a], r.cp[a]);
+        r.apod[a] = (a < g.ndim && g.W[a] != 1) ? p->apod[a] : nullptr;
+    }
+    r.apod_on_output = 1;
+    r.scale = (float)(1.0 / (double)g.gsize);  // ifftn norm="backward"
+    r.nbatch = batch * ncoeff;
+    r.osize = g.isize;
+    r.isize = g.gsize;
+    r.in_real = 0;
+    return launch_resize(r, w.coef, (float2 *)image, st);
+}
+
 extern "C" int dmr_toeplitz_workspace_bytes(int ndim, const int32_t *kshape, int64_t batch, size_t *bytes)
 {
     DMR_CHECK(bytes && batch >= 1, DMR_ERR_INVALID, "bad argument");

@@ -128,6 +128,13 @@ class DevicePlan:
             _lib.check(_lib.lib().dmr_nufft_workspace_bytes(self.handle, int(batch), ctypes.byref(n)))
         return torch.empty(int(n.value), dtype=torch.uint8, device=self.device)
 
+    def workspace_lowrank(self, batch, ncoeff):
+        n = ctypes.c_size_t()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().dmr_nufft_lowrank_workspace_bytes(self.handle, int(batch), int(ncoeff),
+                                                                    ctypes.byref(n)))
+        return torch.empty(int(n.value), dtype=torch.uint8, device=self.device)
+
 
 @dataclass
 class NUFFTPlan:
@@ -372,11 +379,16 @@ def _as_cfloat(x):
 DETERMINISTIC_GRIDDING = False
 
 
-def _check_basis(basis):
-    if basis is not None:
-        raise NotImplementedError(
-            "low-rank subspace NUFFT (basis / basis_adjoint) is not implemented by deepmr_b200"
-        )
+def _basis_arg(basis, rows, cols, dev, name):
+    """Subspace matrix as a contiguous complex64 device tensor of shape (rows, cols)
+    (basis_adjoint: (nframes, ncoeff), indexed [frame, coeff] like the reference's
+    kernels, interp.py:230-357; basis: (ncoeff, nframes), grid.py:287-417)."""
+    b = torch.as_tensor(basis)
+    b = b.to(torch.complex64) if b.is_complex() else b.to(torch.float32).to(torch.complex64)
+    if b.dim() != 2 or (cols is not None and tuple(b.shape) != (rows, cols)) or (cols is None and b.shape[0] != rows):
+        raise ValueError(f"{name} must have shape ({rows}, {cols if cols is not None else 'ncoeff'}), "
+                         f"got {tuple(b.shape)}")
+    return b.to(dev).contiguous()
 
 
 def _sample_dims(interp):
@@ -405,9 +417,10 @@ def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
 
 
 def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblock):
+    if basis_adjoint is not None:
+        return _apply_nufft_lowrank(image, nufft_plan, basis_adjoint, weight, device)
     isnumpy = isinstance(image, np.ndarray)
     image = _as_cfloat(image)
-    _check_basis(basis_adjoint)
     if device is not None:
         nufft_plan.to(device)
     interp = nufft_plan.interpolator
@@ -443,9 +456,10 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
 
 
 def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock, deterministic=None):
+    if basis is not None:
+        return _apply_nufft_adj_lowrank(kspace, nufft_plan, basis, weight, device, deterministic)
     isnumpy = isinstance(kspace, np.ndarray)
     kspace = _as_cfloat(kspace)
-    _check_basis(basis)
     if device is not None:
         nufft_plan.to(device)
     interp = nufft_plan.interpolator
@@ -477,6 +491,78 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
                     _lib.stream_ptr(dev),
                 )
             )
+    out = _to_origin(out, kspace)
+    return out.numpy(force=True) if isnumpy else out
+
+
+def _apply_nufft_lowrank(image, nufft_plan, basis_adjoint, weight, device):
+    """Forward NUFFT of subspace coefficients: image (..., ncoeff, *shape) ->
+    k-space (..., [nframes,] samples), frame f from sum_c basis_adjoint[f, c] image[c]."""
+    isnumpy = isinstance(image, np.ndarray)
+    image = _as_cfloat(image)
+    if device is not None:
+        nufft_plan.to(device)
+    interp = nufft_plan.interpolator
+    dev = interp.device
+    ndim = nufft_plan.ndim
+    nframes = interp.nframes
+    x = image.to(dev)
+    if tuple(x.shape[-ndim:]) != tuple(int(s) for s in nufft_plan.shape) or x.dim() < ndim + 1:
+        raise ValueError(f"image {tuple(x.shape)} must be (..., ncoeff, *{tuple(nufft_plan.shape)})")
+    ncoeff = int(x.shape[-ndim - 1])
+    ba = _basis_arg(basis_adjoint, nframes, ncoeff, dev, "basis_adjoint")
+    batch_shape = x.shape[: -ndim - 1]
+    frames_shape = (nframes,) if nframes > 1 else ()
+    batch = int(np.prod(batch_shape))
+    x = x.contiguous()
+    out = torch.empty(_kspace_shape(interp, batch_shape), dtype=torch.complex64, device=dev)
+    if batch > 0 and interp.total > 0:
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        ws = interp.workspace_lowrank(batch, ncoeff)
+        with torch.cuda.device(dev):
+            _lib.check(_lib.lib().dmr_nufft_forward_lowrank(
+                interp.handle, _lib.ptr(x), int(not x.is_complex()), ncoeff, _lib.ptr(ba), _lib.ptr(out),
+                batch, _lib.ptr(w), wpb, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev)))
+    out = _to_origin(out, image)
+    return out.numpy(force=True) if isnumpy else out
+
+
+def _apply_nufft_adj_lowrank(kspace, nufft_plan, basis, weight, device, deterministic=None):
+    """Adjoint NUFFT onto subspace coefficients: k-space (..., [nframes,] samples)
+    -> image (..., ncoeff, *shape), coefficient c from sum_f basis[c, f] A_f^H y_f."""
+    isnumpy = isinstance(kspace, np.ndarray)
+    kspace = _as_cfloat(kspace)
+    if device is not None:
+        nufft_plan.to(device)
+    interp = nufft_plan.interpolator
+    dev = interp.device
+    nframes = interp.nframes
+    y = kspace.to(dev)
+    nsd = _sample_dims(interp)
+    if nframes == 1 or interp.ishape is None:
+        batch_shape = y.shape[:-nsd]
+    else:
+        batch_shape = y.shape[: -nsd - 1]
+    if list(y.shape) != _kspace_shape(interp, batch_shape):
+        raise ValueError(f"kspace shape {tuple(y.shape)} does not match the plan samples {_sample_shape(interp)}")
+    b = torch.as_tensor(basis)
+    if b.dim() != 2:
+        raise ValueError(f"basis must have shape (ncoeff, {nframes}), got {tuple(b.shape)}")
+    ncoeff = int(b.shape[0])
+    bb = _basis_arg(b, ncoeff, nframes, dev, "basis")
+    frames_shape = (nframes,) if nframes > 1 else ()
+    batch = int(np.prod(batch_shape))
+    y = y.contiguous()
+    out = torch.empty(list(batch_shape) + [ncoeff] + [int(s) for s in nufft_plan.shape],
+                      dtype=torch.complex64, device=dev)
+    if batch > 0:
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        ws = interp.workspace_lowrank(batch, ncoeff)
+        det = int(DETERMINISTIC_GRIDDING if deterministic is None else deterministic)
+        with torch.cuda.device(dev):
+            _lib.check(_lib.lib().dmr_nufft_adjoint_lowrank(
+                interp.handle, _lib.ptr(y), int(not y.is_complex()), ncoeff, _lib.ptr(bb), _lib.ptr(out), batch,
+                _lib.ptr(w), wpb, det, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev)))
     out = _to_origin(out, kspace)
     return out.numpy(force=True) if isnumpy else out
 

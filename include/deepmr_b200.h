@@ -166,6 +166,32 @@ int dmr_nufft_adjoint(dmr_plan *plan, const void *kspace, int kspace_real,
                       void *workspace, size_t workspace_bytes, void *stream);
 
 /*
+ * Low-rank subspace NUFFT. Replaces the basis branches of the reference's
+ * interpolation and gridding (_interpolate_lowrank{1,2,3} /
+ * _gridding_lowrank{1,2,3}, src/deepmr/fft/_interp/interp.py:230-357 and
+ * src/deepmr/fft/_interp/grid.py:287-417, selected by apply_nufft's
+ * basis_adjoint / apply_nufft_adj's basis, src/deepmr/fft/nufft.py:450-606).
+ * Forward: frame f interpolates sum_c basis_adjoint[f, c] * FFT(image[c]);
+ * adjoint: image[c] = crop/apodise(IFFT(sum_f basis[c, f] * grid_f)). The
+ * reference runs only when ncoeff equals the frame count; here any
+ * 1 <= ncoeff <= 32 is accepted.
+ *  image: (batch, ncoeff, *shape); kspace: (batch, total) as above.
+ *  basis_adjoint: device (nframes, ncoeff) complex64; basis: device
+ *  (ncoeff, nframes) complex64 (row-major).
+ */
+int dmr_nufft_lowrank_workspace_bytes(dmr_plan *plan, int64_t batch, int64_t ncoeff,
+                                      size_t *bytes);
+int dmr_nufft_forward_lowrank(dmr_plan *plan, const void *image, int image_real,
+                              int64_t ncoeff, const void *basis_adjoint, void *kspace,
+                              int64_t batch, const float *weight, int weight_per_batch,
+                              void *workspace, size_t workspace_bytes, void *stream);
+int dmr_nufft_adjoint_lowrank(dmr_plan *plan, const void *kspace, int kspace_real,
+                              int64_t ncoeff, const void *basis, void *image,
+                              int64_t batch, const float *weight, int weight_per_batch,
+                              int deterministic, void *workspace, size_t workspace_bytes,
+                              void *stream);
+
+/*
  * Trajectory gradient of the NUFFT. No counterpart in the reference: its
  * autograd returns no coordinate gradient (src/deepmr/fft/nufft.py:188-209).
  *   grad[p, a] = post_scale * sum_b Re(conj(v_b[p]) * dy_b[p] / dcoord[p, a])

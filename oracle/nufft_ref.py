@@ -343,6 +343,28 @@ def apply_nufft_adj(kspace, plan, weight=None):
     return img.numpy() if isnumpy else img
 
 
+def apply_nufft_lowrank(image, plan, basis_adjoint, weight=None):
+    """Low-rank forward (src/deepmr/fft/_interp/interp.py:230-357): frame f is
+    the NUFFT of sum_c basis_adjoint[f, c] image[..., c, :]. Restated through the
+    linearity of apodisation, padding and FFT: combine, then transform."""
+    ndim = plan.ndim
+    ba = torch.as_tensor(basis_adjoint).to(torch.complex64)
+    x = _as_cfloat(torch.as_tensor(image)).to(torch.complex64)
+    xf = torch.einsum("fc,...cn->...fn", ba, x.reshape(*x.shape[: -ndim], -1)).reshape(
+        *x.shape[: -ndim - 1], ba.shape[0], *x.shape[-ndim:])
+    return apply_nufft(xf, plan, weight=weight)
+
+
+def apply_nufft_adj_lowrank(kspace, plan, basis, weight=None):
+    """Low-rank adjoint (src/deepmr/fft/_interp/grid.py:287-417): coefficient c
+    is sum_f basis[c, f] times the adjoint NUFFT of frame f."""
+    ndim = plan.ndim
+    b = torch.as_tensor(basis).to(torch.complex64)
+    xf = apply_nufft_adj(kspace, plan, weight=weight)
+    return torch.einsum("cf,...fn->...cn", b, xf.reshape(*xf.shape[: -ndim], -1)).reshape(
+        *xf.shape[: -ndim - 1], b.shape[0], *xf.shape[-ndim:])
+
+
 def nufft(image, coord, shape=None, width=4, oversamp=1.25):
     """One-shot forward, src/deepmr/fft/__init__.py:145-218."""
     ndim = coord.shape[-1]

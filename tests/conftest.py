@@ -17,9 +17,12 @@ def pytest_configure(config):
 def golden_cases(prefix=None, kind="nufft"):
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     toep = [n for n in names if n.startswith("toep")]
+    lowrank = [n for n in names if n.startswith("lowrank")]
     if kind == "toeplitz":
         return toep
-    return [n for n in names if n not in toep]
+    if kind == "lowrank":
+        return lowrank
+    return [n for n in names if n not in toep and n not in lowrank]
 
 
 @pytest.fixture

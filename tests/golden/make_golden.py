@@ -3,7 +3,8 @@
 Run in a container where the reference project is available (read-only) at
 ``/root/reference``::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every case
+    python tests/golden/make_golden.py lowrank    # only the low-rank cases
 
 The reference's top-level package import needs optional I/O dependencies that
 are absent, so the script registers stub parent packages whose ``__path__``
@@ -112,8 +113,50 @@ def toeplitz_case(N, name, coord, shape, batch_shape, dcf=None, width=4, seed=0)
     print(f"{name}: kernel {np.asarray(T.value).shape} out {tuple(out_img.shape)}")
 
 
+def lowrank_case(N, name, coord, shape, batch_shape, width, oversamp, weight=None, real_basis=False, seed=0):
+    """Low-rank subspace NUFFT with a square basis (ncoeff = nframes, the only
+    case the reference runs): forward with basis_adjoint (nframes, ncoeff),
+    adjoint with basis (ncoeff, nframes)."""
+    coord = torch.as_tensor(coord, dtype=torch.float32)
+    plan = N.plan_nufft(coord, shape, width=width, oversamp=oversamp)
+    ndim = coord.shape[-1]
+    nframes = coord.shape[0]
+    g = torch.Generator().manual_seed(seed)
+    if real_basis:
+        basis = torch.randn(nframes, nframes, generator=g)
+    else:
+        basis = torch.complex(torch.randn(nframes, nframes, generator=g), torch.randn(nframes, nframes, generator=g))
+    basis_adj = basis.conj().t().contiguous()
+    img_shape = list(batch_shape) + [nframes] + list(plan.shape)
+    img = torch.complex(torch.randn(img_shape, generator=g), torch.randn(img_shape, generator=g))
+    ksp_shape = list(batch_shape) + [nframes] + list(plan.interpolator.ishape)
+    ksp = torch.complex(torch.randn(ksp_shape, generator=g), torch.randn(ksp_shape, generator=g))
+    w = None if weight is None else torch.as_tensor(weight, dtype=torch.float32)
+    y = N.apply_nufft(img.clone(), plan, basis_adjoint=basis_adj, weight=w)
+    x = N.apply_nufft_adj(ksp.clone(), plan, basis=basis, weight=w)
+    out = dict(coord=_np(coord), shape=np.asarray(shape), width=np.asarray(width),
+               oversamp=np.asarray(oversamp, dtype=np.float64), image=_np(img), kspace=_np(ksp),
+               basis=_np(basis), basis_adjoint=_np(basis_adj), fwd=_np(y), adj=_np(x), ndim=np.int32(ndim))
+    if w is not None:
+        out["weight"] = _np(w)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: fwd {tuple(y.shape)} adj {tuple(x.shape)}")
+
+
+def lowrank_cases(N):
+    # 2D, 4 frames of rotated radial spokes, complex basis, density weights
+    c = np.stack([synth.radial_2d(6, 20, 16, angle_offset=0.41 * f) for f in range(4)])
+    lowrank_case(N, "lowrank2d", c, 16, [2], 4, 1.25, weight=synth.ramp_dcf(c[0])[None].repeat(4, 0))
+    # 3D, 3 frames, real basis
+    c = np.stack([synth.kooshball_3d(20, 12, 8) * (1.0 - 0.1 * f) for f in range(3)]).astype(np.float32)
+    lowrank_case(N, "lowrank3d", c, 8, [1], 4, 1.25, real_basis=True, seed=1)
+
+
 def main():
     N, _ = import_reference()
+    if sys.argv[1:] == ["lowrank"]:
+        lowrank_cases(N)
+        return
 
     # 2D golden-angle radial, width 3 / oversampling 2 (the 2D benchmark's kernel)
     c = synth.radial_2d(16, 32, 32)
@@ -173,6 +216,8 @@ def main():
     toeplitz_case(N, "toep2d_frames", c, 10, [2])
     c = synth.kooshball_3d(30, 16, 8)
     toeplitz_case(N, "toep3d", c, 8, [2], dcf=synth.ramp_dcf(c))
+
+    lowrank_cases(N)
 
 
 if __name__ == "__main__":

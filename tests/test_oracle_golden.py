@@ -66,6 +66,19 @@ def test_oracle_toeplitz(name, load_golden):
     assert R.rel_l2(out, g["selfadj"]) < TOL
 
 
+@pytest.mark.parametrize("name", golden_cases(kind="lowrank"))
+def test_oracle_lowrank(name, load_golden):
+    """Low-rank subspace NUFFT (square basis: the reference runs only then)."""
+    g = load_golden(name)
+    plan = R.plan_nufft(torch.as_tensor(g["coord"]), _shape(g), _width(g), _os(g))
+    w = g.get("weight")
+    y = R.apply_nufft_lowrank(torch.as_tensor(g["image"]), plan, g["basis_adjoint"], weight=w)
+    x = R.apply_nufft_adj_lowrank(torch.as_tensor(g["kspace"]), plan, g["basis"], weight=w)
+    assert tuple(y.shape) == g["fwd"].shape and tuple(x.shape) == g["adj"].shape
+    assert R.rel_l2(y, g["fwd"]) < TOL
+    assert R.rel_l2(x, g["adj"]) < TOL
+
+
 def test_oracle_vs_nudft_small():
     """The reference operator approximates the exact NUDFT (expected error ~1e-2 at W3/os2)."""
     from deepmr_b200 import synth
