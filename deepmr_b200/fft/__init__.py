@@ -1,7 +1,8 @@
 """Non-Cartesian NUFFT on B200 — drop-in for ``deepmr.fft``'s NUFFT API.
 
-One-shot ``nufft`` / ``nufft_adj`` (reference: src/deepmr/fft/__init__.py:145-286)
-and the plan/apply functions of ``deepmr.fft.nufft``.
+One-shot ``nufft`` / ``nufft_adj`` and ``sparse_fft`` / ``sparse_ifft``
+(reference: src/deepmr/fft/__init__.py:31-286), the plan/apply functions of
+``deepmr.fft.nufft`` and of ``deepmr.fft.sparse_fft``.
 """
 
 import torch
@@ -17,6 +18,15 @@ from .nufft import (  # noqa: F401
     plan_toeplitz_nufft,
 )
 from .graphs import CapturedNUFFT, frames_concat, frames_split  # noqa: F401
+from . import sparse_fft as _sparse_fft
+from .sparse_fft import (  # noqa: F401
+    SparseSampling,
+    apply_sparse_fft,
+    apply_sparse_fft_selfadj,
+    apply_sparse_ifft,
+    plan_toeplitz_fft,
+    prepare_sampling,
+)
 from .nufft import traj_grad  # noqa: F401
 from .toeplitz import GramMatrix  # noqa: F401
 
@@ -36,6 +46,14 @@ __all__ = [
     "CapturedNUFFT",
     "frames_split",
     "frames_concat",
+    "sparse_fft",
+    "sparse_ifft",
+    "prepare_sampling",
+    "plan_toeplitz_fft",
+    "apply_sparse_fft",
+    "apply_sparse_ifft",
+    "apply_sparse_fft_selfadj",
+    "SparseSampling",
 ]
 
 
@@ -86,3 +104,16 @@ def nufft_adj(kspace, coord, shape, basis=None, device="cpu", threadsperblock=12
         return _nufft.NUFFTAdjTraj.apply(_nufft._as_cfloat(kspace), coord, shape, width, oversamp, device, None)
     plan = _nufft.plan_nufft(coord, shape, width, oversamp, device)
     return _nufft.apply_nufft_adj(kspace, plan, basis, threadsperblock=threadsperblock)
+
+
+def sparse_fft(image, indexes, basis_adjoint=None, device="cpu", threadsperblock=128):
+    """Sparse FFT, plan + apply (reference: src/deepmr/fft/__init__.py:31-86)."""
+    ndim = indexes.shape[-1]
+    mask = _sparse_fft.prepare_sampling(indexes, image.shape[-ndim:], device)
+    return _sparse_fft.apply_sparse_fft(image, mask, basis_adjoint, threadsperblock=threadsperblock)
+
+
+def sparse_ifft(kspace, indexes, shape, basis=None, device="cpu", threadsperblock=128):
+    """Inverse sparse FFT, plan + apply (reference: src/deepmr/fft/__init__.py:89-142)."""
+    mask = _sparse_fft.prepare_sampling(indexes, shape, device)
+    return _sparse_fft.apply_sparse_ifft(kspace, mask, basis, threadsperblock=threadsperblock)

@@ -525,3 +525,89 @@ class Forward64:
                 index.append(taps[a][i])
             acc = acc + w * self.K[(...,) + tuple(index[::-1])]
         return acc / self.scale
+
+
+# ---------------------------------------------------------------------------
+# Cartesian sparse FFT (src/deepmr/fft/sparse_fft.py, src/deepmr/fft/_sparse/*)
+# ---------------------------------------------------------------------------
+def _sparse_index(indexes, ndim):
+    idx = np.asarray(indexes).astype(np.int64)
+    ish = list(idx.shape[:-1])
+    while len(ish) < 3:
+        ish = [1] + ish
+    return idx.reshape(ish[0], -1, ndim), ish[0], tuple(ish[1:])
+
+
+def _centred_fft(x, ndim, inverse=False):
+    ax = tuple(range(-ndim, 0))
+    x = np.fft.ifftshift(x, axes=ax)
+    x = np.fft.ifftn(x, axes=ax) if inverse else np.fft.fftn(x, axes=ax)
+    return np.fft.fftshift(x, axes=ax)
+
+
+def sparse_fft(image, indexes, shape, basis_adjoint=None, weight=None):
+    """Centred FFT (unnormalised) then sampling at integer indexes
+    (sparse_fft.py:314-383, _sparse/dense2sparse.py); frames as the NUFFT."""
+    ndim = np.asarray(indexes).shape[-1]
+    idx, nframes, ishape = _sparse_index(indexes, ndim)
+    x = np.asarray(image, dtype=np.complex128)
+    if basis_adjoint is not None:
+        x = np.einsum("fc,...cn->...fn", np.asarray(basis_adjoint), x.reshape(*x.shape[:-ndim], -1)).reshape(
+            *x.shape[: -ndim - 1], nframes, *x.shape[-ndim:])
+    X = _centred_fft(x, ndim)
+    lead = X.shape[: -ndim - 1] if nframes > 1 else X.shape[:-ndim]
+    X = X.reshape(-1, nframes, *X.shape[-ndim:])
+    out = np.empty((X.shape[0], nframes, idx.shape[1]), np.complex128)
+    for f in range(nframes):
+        sel = tuple(idx[f, :, a] for a in range(ndim))[::-1]  # (z, y, x) order
+        out[:, f] = X[(slice(None), f) + sel]
+    if weight is not None:
+        out = out * np.asarray(weight, np.float64).reshape(1, nframes, -1)
+    shape_out = list(lead) + ([nframes] if nframes > 1 else []) + list(ishape)
+    return out.reshape(shape_out).astype(np.complex64)
+
+
+def sparse_ifft(kspace, indexes, shape, basis=None, weight=None):
+    """Zero-fill (repeated indexes summed) then centred inverse FFT (1/N)
+    (sparse_fft.py:386-450, _sparse/sparse2dense.py)."""
+    ndim = np.asarray(indexes).shape[-1]
+    idx, nframes, ishape = _sparse_index(indexes, ndim)
+    sh = [int(shape)] * ndim if np.isscalar(shape) else [int(s) for s in shape]
+    y = np.asarray(kspace, dtype=np.complex128)
+    lead = y.shape[: -len(ishape) - 1] if nframes > 1 else y.shape[: -len(ishape)]
+    y = y.reshape(-1, nframes, idx.shape[1])
+    if weight is not None:
+        y = y * np.asarray(weight, np.float64).reshape(1, nframes, -1)
+    grid = np.zeros((y.shape[0], nframes, *sh), np.complex128)
+    for f in range(nframes):
+        sel = tuple(idx[f, :, a] for a in range(ndim))[::-1]
+        for b in range(y.shape[0]):
+            np.add.at(grid[b, f], sel, y[b, f])
+    x = _centred_fft(grid, ndim, inverse=True)
+    if basis is not None:
+        x = np.einsum("cf,bfn->bcn", np.asarray(basis), x.reshape(x.shape[0], nframes, -1)).reshape(
+            x.shape[0], -1, *sh)
+        return x.reshape(list(lead) + [x.shape[1]] + sh).astype(np.complex64)
+    return x.reshape(list(lead) + ([nframes] if nframes > 1 else []) + sh).astype(np.complex64)
+
+
+def sparse_toeplitz_kernel(indexes, shape):
+    """Sample counts per k-space point, ifftshifted and normalised (_sparse/toeplitz.py:15-113)."""
+    ndim = np.asarray(indexes).shape[-1]
+    idx, nframes, _ = _sparse_index(indexes, ndim)
+    sh = [int(shape)] * ndim if np.isscalar(shape) else [int(s) for s in shape]
+    k = np.zeros((nframes, *sh), np.float64)
+    for f in range(nframes):
+        np.add.at(k[f], tuple(idx[f, :, a] for a in range(ndim))[::-1], 1.0)
+    k = np.fft.ifftshift(k, axes=tuple(range(-ndim, 0)))
+    k = k if nframes > 1 else k[0]
+    # normalised by the mean non-zero magnitude, NaN -> 0 (_sparse/toeplitz.py:107-111)
+    nz = k[k != 0]
+    return np.nan_to_num(k / (np.abs(nz).mean() if nz.size else np.nan))
+
+
+def sparse_selfadj(image, kernel, ndim):
+    """Uncentred orthonormal FFT, times the kernel, inverse (sparse_fft.py:453-503)."""
+    ax = tuple(range(-ndim, 0))
+    X = np.fft.fftn(np.asarray(image, np.complex128), axes=ax, norm="ortho")
+    return np.fft.ifftn(X * np.asarray(kernel), axes=ax, norm="ortho").astype(np.complex64)

@@ -18,11 +18,14 @@ def golden_cases(prefix=None, kind="nufft"):
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     toep = [n for n in names if n.startswith("toep")]
     lowrank = [n for n in names if n.startswith("lowrank")]
+    sparse = [n for n in names if n.startswith("sparse")]
     if kind == "toeplitz":
         return toep
     if kind == "lowrank":
         return lowrank
-    return [n for n in names if n not in toep and n not in lowrank]
+    if kind == "sparse":
+        return sparse
+    return [n for n in names if n not in toep and n not in lowrank and n not in sparse]
 
 
 @pytest.fixture

@@ -5,6 +5,7 @@ Run in a container where the reference project is available (read-only) at
 
     python tests/golden/make_golden.py            # every case
     python tests/golden/make_golden.py lowrank    # only the low-rank cases
+    python tests/golden/make_golden.py sparse     # only the sparse FFT cases
 
 The reference's top-level package import needs optional I/O dependencies that
 are absent, so the script registers stub parent packages whose ``__path__``
@@ -152,10 +153,66 @@ def lowrank_cases(N):
     lowrank_case(N, "lowrank3d", c, 8, [1], 4, 1.25, real_basis=True, seed=1)
 
 
+def sparse_case(S, name, indexes, shape, batch_shape, weight=None, basis=False, seed=0):
+    """Cartesian sparse FFT (src/deepmr/fft/sparse_fft.py): forward, adjoint,
+    self-adjoint (Toeplitz counts; not with a basis) on seeded inputs."""
+    idx = torch.as_tensor(indexes, dtype=torch.int16)
+    mask = S.prepare_sampling(idx, shape)
+    ndim = idx.shape[-1]
+    nframes = idx.shape[0] if idx.ndim == 4 else 1
+    sh = [shape] * ndim if np.isscalar(shape) else list(shape)
+    g = torch.Generator().manual_seed(seed)
+    b = ba = None
+    if basis:
+        b = torch.complex(torch.randn(nframes, nframes, generator=g), torch.randn(nframes, nframes, generator=g))
+        ba = b.conj().t().contiguous()
+    img_shape = list(batch_shape) + ([nframes] if nframes > 1 else []) + sh
+    img = torch.complex(torch.randn(img_shape, generator=g), torch.randn(img_shape, generator=g))
+    y = S.apply_sparse_fft(img.clone(), mask, basis_adjoint=ba,
+                           weight=None if weight is None else torch.as_tensor(weight, dtype=torch.float32))
+    ksp = torch.complex(torch.randn(tuple(y.shape), generator=g), torch.randn(tuple(y.shape), generator=g))
+    x = S.apply_sparse_ifft(ksp.clone(), mask, basis=b,
+                            weight=None if weight is None else torch.as_tensor(weight, dtype=torch.float32))
+    out = dict(indexes=_np(idx), shape=np.asarray(shape), image=_np(img), kspace=_np(ksp), fwd=_np(y), adj=_np(x),
+               ndim=np.int32(ndim))
+    if weight is not None:
+        out["weight"] = np.asarray(weight, np.float32)
+    if basis:
+        out["basis"] = _np(b)
+        out["basis_adjoint"] = _np(ba)
+    else:
+        T = S.plan_toeplitz_fft(idx, shape)
+        out["kernel"] = _np(T.value)
+        out["selfadj"] = _np(S.apply_sparse_fft_selfadj(img.clone(), T))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(f"{name}: fwd {tuple(y.shape)} adj {tuple(x.shape)}")
+
+
+def sparse_cases():
+    S = sys.modules["deepmr.fft.sparse_fft"]
+    rng = np.random.default_rng(7)
+    # 2D, 3 frames, repeated indexes, per-sample weights
+    idx = rng.integers(0, 12, size=(3, 5, 8, 2))
+    idx[0, 0, :3] = idx[0, 0, 3]
+    sparse_case(S, "sparse2d", idx, 12, [2], weight=rng.uniform(0.2, 1.0, (3, 5, 8)))
+    # 2D anisotropic grid (10, 14), single frame
+    idx = np.stack([rng.integers(0, 14, (6, 9)), rng.integers(0, 10, (6, 9))], -1)
+    sparse_case(S, "sparse2d_aniso", idx, (10, 14), [3], seed=1)
+    # 3D single frame
+    idx = rng.integers(0, 8, size=(4, 10, 3))
+    sparse_case(S, "sparse3d", idx, 8, [2], seed=2)
+    # 2D, 3 frames, square complex subspace basis
+    idx = rng.integers(0, 10, size=(3, 4, 6, 2))
+    sparse_case(S, "sparse2d_lowrank", idx, 10, [2], basis=True, seed=3)
+
+
 def main():
     N, _ = import_reference()
     if sys.argv[1:] == ["lowrank"]:
         lowrank_cases(N)
+        return
+    if sys.argv[1:] == ["sparse"]:
+        sparse_cases()
         return
 
     # 2D golden-angle radial, width 3 / oversampling 2 (the 2D benchmark's kernel)
@@ -218,6 +275,7 @@ def main():
     toeplitz_case(N, "toep3d", c, 8, [2], dcf=synth.ramp_dcf(c))
 
     lowrank_cases(N)
+    sparse_cases()
 
 
 if __name__ == "__main__":

@@ -79,6 +79,23 @@ def test_oracle_lowrank(name, load_golden):
     assert R.rel_l2(x, g["adj"]) < TOL
 
 
+@pytest.mark.parametrize("name", golden_cases(kind="sparse"))
+def test_oracle_sparse_fft(name, load_golden):
+    """Cartesian sparse FFT: forward, adjoint (repeated indexes), self-adjoint."""
+    g = load_golden(name)
+    shape = int(g["shape"]) if g["shape"].ndim == 0 else tuple(int(s) for s in g["shape"])
+    w = g.get("weight")
+    y = R.sparse_fft(g["image"], g["indexes"], shape, g.get("basis_adjoint"), weight=w)
+    x = R.sparse_ifft(g["kspace"], g["indexes"], shape, g.get("basis"), weight=w)
+    assert y.shape == g["fwd"].shape and x.shape == g["adj"].shape
+    assert R.rel_l2(y, g["fwd"]) < TOL
+    assert R.rel_l2(x, g["adj"]) < TOL
+    if "kernel" in g:
+        k = R.sparse_toeplitz_kernel(g["indexes"], shape)
+        np.testing.assert_allclose(k, g["kernel"], rtol=1e-6, atol=1e-7)
+        assert R.rel_l2(R.sparse_selfadj(g["image"], k, int(g["ndim"])), g["selfadj"]) < TOL
+
+
 def test_oracle_vs_nudft_small():
     """The reference operator approximates the exact NUDFT (expected error ~1e-2 at W3/os2)."""
     from deepmr_b200 import synth
