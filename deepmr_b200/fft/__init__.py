@@ -9,6 +9,7 @@ import torch
 
 from . import nufft as _nufft
 from . import toeplitz as _toeplitz
+from .fft import fft, ifft  # noqa: F401
 from .nufft import (  # noqa: F401
     NUFFTPlan,
     apply_nufft,
@@ -31,6 +32,8 @@ from .nufft import traj_grad  # noqa: F401
 from .toeplitz import GramMatrix  # noqa: F401
 
 __all__ = [
+    "fft",
+    "ifft",
     "nufft",
     "nufft_adj",
     "plan_nufft",

@@ -1,0 +1,20 @@
+"""Centred fft / ifft of the package (the reference's src/deepmr/fft/fft.py
+semantics: fftshift(fftn(ifftshift(x))) with norm, over the given axes)."""
+
+import numpy as np
+import torch
+
+
+def test_centred_fft_matches_numpy_and_round_trips():
+    import deepmr_b200.fft as F
+
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal((3, 6, 5)) + 1j * rng.standard_normal((3, 6, 5))).astype(np.complex64)
+    ax = (-2, -1)
+    ref = np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(x, axes=ax), axes=ax, norm="ortho"), axes=ax)
+    y = F.fft(x, axes=ax)
+    assert isinstance(y, np.ndarray)
+    np.testing.assert_allclose(y, ref, rtol=1e-5, atol=1e-5)
+    np.testing.assert_allclose(F.ifft(y, axes=ax), x, rtol=1e-5, atol=1e-5)
+    t = F.fft(torch.as_tensor(x), axes=(1,), norm=None, centered=False)
+    np.testing.assert_allclose(t.numpy(), np.fft.fft(x, axis=1), rtol=1e-4, atol=1e-4)
