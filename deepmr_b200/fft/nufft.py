@@ -416,6 +416,92 @@ def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
     return torch.broadcast_to(w, _kspace_shape(interp, batch_shape)).contiguous(), 1
 
 
+# Pinned host inputs of at least this many bytes (input + output) run through a
+# chunked pipeline: the copy in of one chunk of the batch, the compute of the
+# previous chunk and the copy out of the one before overlap (H2D and D2H run on
+# separate copy engines), instead of copy in -> compute -> copy out in series.
+PIPELINE_MIN_BYTES = 64 << 20
+PIPELINE_CHUNKS = 8
+
+_PIPE_STREAMS = {}
+
+
+def _pipe_streams(dev):
+    """(copy-in, compute, copy-out) streams of ``dev``, created once."""
+    key = dev.index if dev.index is not None else torch.cuda.current_device()
+    s = _PIPE_STREAMS.get(key)
+    if s is None:
+        with torch.cuda.device(key):
+            s = (torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream())
+        _PIPE_STREAMS[key] = s
+    return s
+
+
+def _pipelinable(host, dev, batch, out_item_bytes):
+    """True for a pinned, contiguous CPU input whose batch is worth chunking."""
+    if dev.type != "cuda" or host.device.type != "cpu" or batch < 2:
+        return False
+    if not (host.is_contiguous() and host.is_pinned()):
+        return False
+    nbytes = host.numel() * host.element_size() + batch * out_item_bytes
+    return nbytes >= PIPELINE_MIN_BYTES
+
+
+def _pipelined(x_h, out_h, batch, dev, run, ws_bytes):
+    """Run ``run(x_dev, out_dev, b0, nb, ws, stream)`` over chunks of the
+    flattened batch: ``x_h`` (batch, ...) and ``out_h`` (batch, ...) are pinned
+    host tensors, device input/output buffers are double-buffered, and the
+    compute stream runs the chunks in order with one workspace. Returns after
+    every copy out has completed (``out_h`` is then valid on the host)."""
+    nch = min(batch, PIPELINE_CHUNKS)
+    cb = -(-batch // nch)
+    nch = -(-batch // cb)
+    h2d, comp, d2h = _pipe_streams(dev)
+    with torch.cuda.device(dev):
+        cur = torch.cuda.current_stream(dev)
+        xb = [torch.empty((cb,) + tuple(x_h.shape[1:]), dtype=x_h.dtype, device=dev) for _ in range(min(2, nch))]
+        ob = [torch.empty((cb,) + tuple(out_h.shape[1:]), dtype=out_h.dtype, device=dev) for _ in range(min(2, nch))]
+        ws = ws_bytes(cb)
+        start = torch.cuda.Event()
+        start.record(cur)
+        for s in (h2d, comp, d2h):
+            s.wait_event(start)
+        ev_in = [torch.cuda.Event() for _ in range(nch)]
+        ev_comp = [torch.cuda.Event() for _ in range(nch)]
+        ev_out = [torch.cuda.Event() for _ in range(nch)]
+        try:
+            for i in range(nch):
+                b0 = i * cb
+                nb = min(cb, batch - b0)
+                k = i % 2
+                if i >= 2:
+                    h2d.wait_event(ev_comp[i - 2])  # xb[k] is free once chunk i-2 is computed
+                with torch.cuda.stream(h2d):
+                    xb[k][:nb].copy_(x_h[b0:b0 + nb], non_blocking=True)
+                ev_in[i].record(h2d)
+                comp.wait_event(ev_in[i])
+                if i >= 2:
+                    comp.wait_event(ev_out[i - 2])  # ob[k] is free once chunk i-2 is copied out
+                run(xb[k][:nb], ob[k][:nb], b0, nb, ws, ctypes.c_void_p(comp.cuda_stream))
+                ev_comp[i].record(comp)
+                d2h.wait_event(ev_comp[i])
+                with torch.cuda.stream(d2h):
+                    out_h[b0:b0 + nb].copy_(ob[k][:nb], non_blocking=True)
+                ev_out[i].record(d2h)
+        finally:
+            for s in (h2d, comp, d2h):
+                s.synchronize()
+    return out_h
+
+
+def _weight_chunk(w, wpb, b0, nb, batch):
+    """Rows b0 .. b0+nb of per-batch weights (flattened batch); shared weights as they are."""
+    if w is None or not wpb:
+        return w
+    per = w.numel() // batch
+    return w.reshape(-1)[b0 * per:(b0 + nb) * per]
+
+
 def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblock):
     if basis_adjoint is not None:
         return _apply_nufft_lowrank(image, nufft_plan, basis_adjoint, weight, device)
@@ -427,30 +513,40 @@ def _apply_nufft(image, nufft_plan, basis_adjoint, weight, device, threadsperblo
     dev = interp.device
     ndim = nufft_plan.ndim
     nframes = interp.nframes
-    x = image.to(dev)
     if nframes == 1:
-        batch_shape = x.shape[:-ndim]
+        batch_shape = image.shape[:-ndim]
         frames_shape = ()
     else:
-        batch_shape = x.shape[: -ndim - 1]
+        batch_shape = image.shape[: -ndim - 1]
         frames_shape = (nframes,)
-        if x.shape[-ndim - 1] != nframes:
-            raise ValueError(f"expected {nframes} frames before the spatial axes, got {tuple(x.shape)}")
-    if tuple(x.shape[-ndim:]) != tuple(int(s) for s in nufft_plan.shape):
-        raise ValueError(f"image spatial shape {tuple(x.shape[-ndim:])} != plan shape {nufft_plan.shape}")
+        if image.shape[-ndim - 1] != nframes:
+            raise ValueError(f"expected {nframes} frames before the spatial axes, got {tuple(image.shape)}")
+    if tuple(image.shape[-ndim:]) != tuple(int(s) for s in nufft_plan.shape):
+        raise ValueError(f"image spatial shape {tuple(image.shape[-ndim:])} != plan shape {nufft_plan.shape}")
     batch = int(np.prod(batch_shape))
-    x = x.contiguous()
-    out = torch.empty(_kspace_shape(interp, batch_shape), dtype=torch.complex64, device=dev)
+    kshape = _kspace_shape(interp, batch_shape)
+    real = int(not image.is_complex())
+
+    def run(xd, od, b0, nb, ws, stream):
+        _lib.check(
+            _lib.lib().dmr_nufft_forward(
+                interp.handle, _lib.ptr(xd), real, _lib.ptr(od), nb,
+                _lib.ptr(_weight_chunk(w, wpb, b0, nb, batch)), wpb, _lib.ptr(ws), ws.numel(), stream,
+            )
+        )
+
+    if interp.total > 0 and _pipelinable(image, dev, batch, 8 * interp.total):
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        out = torch.empty([batch] + kshape[len(batch_shape):], dtype=torch.complex64, pin_memory=True)
+        _pipelined(image.reshape((batch,) + tuple(image.shape[len(batch_shape):])), out, batch, dev, run,
+                   interp.workspace)
+        return out.reshape(kshape)
+    x = image.to(dev).contiguous()
+    out = torch.empty(kshape, dtype=torch.complex64, device=dev)
     if batch > 0 and interp.total > 0:
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
-        ws = interp.workspace(batch)
         with torch.cuda.device(dev):
-            _lib.check(
-                _lib.lib().dmr_nufft_forward(
-                    interp.handle, _lib.ptr(x), int(not x.is_complex()), _lib.ptr(out), batch,
-                    _lib.ptr(w), wpb, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev),
-                )
-            )
+            run(x, out, 0, batch, interp.workspace(batch), _lib.stream_ptr(dev))
     out = _to_origin(out, image)
     return out.numpy(force=True) if isnumpy else out
 
@@ -464,33 +560,40 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
         nufft_plan.to(device)
     interp = nufft_plan.interpolator
     dev = interp.device
-    ndim = nufft_plan.ndim
     nframes = interp.nframes
-    y = kspace.to(dev)
     nsd = _sample_dims(interp)
     frames_shape = (nframes,) if nframes > 1 else ()
     if nframes == 1 or interp.ishape is None:
-        batch_shape = y.shape[:-nsd]
+        batch_shape = kspace.shape[:-nsd]
     else:
-        batch_shape = y.shape[: -nsd - 1]
-    if list(y.shape) != _kspace_shape(interp, batch_shape):
-        raise ValueError(f"kspace shape {tuple(y.shape)} does not match the plan samples {_sample_shape(interp)}")
+        batch_shape = kspace.shape[: -nsd - 1]
+    if list(kspace.shape) != _kspace_shape(interp, batch_shape):
+        raise ValueError(f"kspace shape {tuple(kspace.shape)} does not match the plan samples {_sample_shape(interp)}")
     batch = int(np.prod(batch_shape))
-    y = y.contiguous()
-    out = torch.empty(list(batch_shape) + list(frames_shape) + [int(s) for s in nufft_plan.shape],
-                      dtype=torch.complex64, device=dev)
+    item = list(frames_shape) + [int(s) for s in nufft_plan.shape]
+    real = int(not kspace.is_complex())
+    det = int(DETERMINISTIC_GRIDDING if deterministic is None else deterministic)
+
+    def run(yd, od, b0, nb, ws, stream):
+        _lib.check(
+            _lib.lib().dmr_nufft_adjoint(
+                interp.handle, _lib.ptr(yd), real, _lib.ptr(od), nb,
+                _lib.ptr(_weight_chunk(w, wpb, b0, nb, batch)), wpb, det, _lib.ptr(ws), ws.numel(), stream,
+            )
+        )
+
+    if _pipelinable(kspace, dev, batch, 8 * int(np.prod(item))):
+        w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
+        out = torch.empty([batch] + item, dtype=torch.complex64, pin_memory=True)
+        _pipelined(kspace.reshape((batch,) + tuple(kspace.shape[len(batch_shape):])), out, batch, dev, run,
+                   interp.workspace)
+        return out.reshape(list(batch_shape) + item)
+    y = kspace.to(dev).contiguous()
+    out = torch.empty(list(batch_shape) + item, dtype=torch.complex64, device=dev)
     if batch > 0:
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
-        ws = interp.workspace(batch)
         with torch.cuda.device(dev):
-            _lib.check(
-                _lib.lib().dmr_nufft_adjoint(
-                    interp.handle, _lib.ptr(y), int(not y.is_complex()), _lib.ptr(out), batch,
-                    _lib.ptr(w), wpb, int(DETERMINISTIC_GRIDDING if deterministic is None else deterministic),
-                    _lib.ptr(ws), ws.numel(),
-                    _lib.stream_ptr(dev),
-                )
-            )
+            run(y, out, 0, batch, interp.workspace(batch), _lib.stream_ptr(dev))
     out = _to_origin(out, kspace)
     return out.numpy(force=True) if isnumpy else out
 
