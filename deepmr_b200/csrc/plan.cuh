@@ -69,6 +69,10 @@ std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t bat
 bool rt_geometry_ok(const Geom &g);
 int rt_build(::dmr_plan *p, const std::vector<int32_t> &h_start, cudaStream_t st);
 size_t rt_scratch_bytes(const ::dmr_plan *p, int64_t batch);
+// tensor-core atomic gridding of 3D plans (tcgrid.cu); DMR_ERR_UNSUPPORTED when
+// the bin region does not fit
+int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                     const float *weight, int wpb, cudaStream_t st);
 
 }  // namespace dmr
 

@@ -1395,6 +1395,11 @@ int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, i
         const int rc = grid_rt_dispatch(p, ksp, kreal, grid, batch, weight, wpb, scratch, scratch_bytes, st);
         if (rc != DMR_ERR_UNSUPPORTED) return rc;
     }
+    // atomic 3D gridding: tensor-core spreading when the bin region fits
+    if (!det && p->g.ndim == 3 && grid_variant() == 0) {
+        const int rc = grid_tc_dispatch(p, ksp, kreal, grid, batch, weight, wpb, st);
+        if (rc != DMR_ERR_UNSUPPORTED) return rc;
+    }
     const int cw = cube_width(p->g);
     if (cw > 0 && (det || (p->g.ndim == 3 && grid_variant() == 1))) {
         switch (p->g.ndim * 100 + cw) {

@@ -1,0 +1,457 @@
+// Tensor-core gridding for 3D (tcgen05, TF32 operands with a three-term split).
+//
+// Reference: apply_gridding and its 3D kernel
+// (src/deepmr/fft/_interp/grid.py:14-125, 253-284):
+//   grid[f, b, iz, iy, ix] += value_z * value_y * value_x * y[f, b, p]   (then / scale)
+//
+// For one bin and a chunk of up to 32 coils, what the bin's samples add to its
+// tile + halo (P = R0 R1 R2 points, R = T + W - 1 per axis) is a matrix product
+//     D[p, n] = sum_s A[p, s] B[n, s]
+// with A[p, s] = wx * wy * wz of sample s at point p (zero outside its W^3
+// support) and B[n, s] the real (n = 2c) or imaginary (n = 2c + 1) part of the
+// value of sample s for coil c. A block builds A and B in shared memory for
+// eight samples at a time and one thread issues tcgen05.mma into a tensor-memory
+// accumulator of M = 128 points x N = 2 x coils per 128-point tile; the
+// accumulator stays in tensor memory for all the samples of the bin, and is
+// then read back (tcgen05.ld) and added to the grid with global float2 atomics.
+// The spreading weights are built once per sample for all coils of the chunk,
+// and the zeros of A cost tensor-core cycles instead of scalar instructions.
+//
+// Precision: each float32 operand x is split into hi (x with the mantissa
+// bits below tf32 cleared) and lo = x - hi, stored as two K blocks [hi | lo];
+// three MMAs per 128-point tile add hi*hi, hi*lo and lo*hi, which leaves a
+// relative error of about 2^-20 per product (the dropped lo*lo term and the
+// tf32 reading of lo), and the accumulation is float32 in tensor memory.
+//
+// Operand layout (K-major, no swizzle): element (r, k) of an operand with K
+// extent 16 is at byte (r / 8) * 512 + (k / 4) * 128 + (r % 8) * 16 + (k % 4) * 4,
+// i.e. 8-row x 16-byte core matrices, adjacent along K (leading byte offset
+// 128) and 512 bytes apart along M / N (stride byte offset 512); k < 8 holds
+// the hi parts of the chunk's eight samples, k >= 8 the lo parts. One MMA takes
+// K = 8 (two core matrices along K).
+//
+// Pipeline: A and B are double-buffered; the MMAs of one chunk run while the
+// threads build the next, and a buffer is rebuilt only after the mbarrier
+// signalled by tcgen05.commit for the chunk that last read it. Every wait is
+// bounded: a wait that runs out sets a device flag, and the block stops
+// issuing work and frees its tensor memory.
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+
+#include "kb.cuh"
+#include "plan.cuh"
+
+namespace dmr {
+
+constexpr int kTcThreads = 384;       // 12 warps; warps 0-7 read the accumulator (two per lane quarter)
+constexpr int kTcSC = 8;              // samples per MMA chunk
+constexpr int kTcK = 2 * kTcSC;       // K extent of a chunk in shared memory ([hi | lo])
+constexpr int kTcSB = 128;            // samples staged per pass
+constexpr int kTcSBP = kTcSB + 4;     // padded row of a staged weight vector (bank spread)
+constexpr int kTcMaxMT = 4;           // 128-point tiles (P <= 512)
+constexpr int kTcMaxCC = 32;          // coils per block (N <= 64)
+static_assert(kTcMaxCC * kTcSC <= kTcThreads, "one (coil, sample) of a chunk per thread");
+constexpr int kTcPairs = (2 * kTcMaxMT * 128 + kTcThreads - 1) / kTcThreads;  // A-build pairs per thread
+constexpr int kTcRowBytes = kTcK * 32;        // 512: stride between 8-row core-matrix groups
+constexpr int kTcTileBytes = 16 * kTcRowBytes;  // 8192: one 128-row operand tile
+constexpr long long kTcSpin = 1ll << 20;      // bound on mbarrier polls
+
+__device__ int g_tc_timeouts = 0;  // waits that ran out (should stay 0)
+
+__device__ __forceinline__ uint32_t tc_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t addr)
+{
+    // start address, leading byte offset 128, stride byte offset 512, version 1, no swizzle
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)(kTcRowBytes >> 4) << 32) | (1ull << 46);
+}
+
+// hi part of the split: x with the 13 mantissa bits that tf32 drops cleared
+// (exactly representable, so lo = x - hi is exact and |lo| < 2^-10 |x|)
+__device__ __forceinline__ float tc_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+__device__ __forceinline__ float4 tc_lds4(uint32_t a)
+{
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+
+__device__ __forceinline__ void tc_sts4(uint32_t a, float4 v)
+{
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_sts(uint32_t a, float v)
+{
+    asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
+__device__ __forceinline__ bool tc_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait for completion number k (parity k & 1) of an mbarrier
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t k)
+{
+    for (long long i = 0; i < kTcSpin; i++)
+        if (tc_try_wait(bar, k & 1)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+struct TcShape {
+    int R[3];    // region extents (T + W - 1)
+    int P;       // points of the region
+    int MT;      // 128-point tiles
+    int N;       // accumulator columns per tile (2 x coils, multiple of 32)
+    int ncols;   // tensor-memory columns allocated (power of two >= MT * N)
+    int CC;      // coils per block
+};
+
+// dynamic shared memory: A[2] | B[2] | staged weight vectors | global sample indices
+__host__ __device__ inline size_t tc_smem_bytes(const TcShape &s)
+{
+    return (size_t)2 * s.MT * kTcTileBytes + (size_t)2 * s.N * (kTcK * 4) +
+           (size_t)(s.R[0] + s.R[1] + s.R[2]) * kTcSBP * 4 + (size_t)kTcSB * 4;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
+    Geom g, TcShape sh, const WorkItem *__restrict__ work, int nwork, int nchunks,
+    const float *__restrict__ sc0, const float *__restrict__ sc1, const float *__restrict__ sc2,
+    const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid,
+    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tslot;
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int W = g.W[0];
+    // buffer b of A at smem + b * MT * 8192, of B at bbase + b * N * 64
+    unsigned char *bbase = smem + 2 * sh.MT * kTcTileBytes;
+    float *vec = reinterpret_cast<float *>(bbase + 2 * sh.N * (kTcK * 4));
+    float *vx = vec, *vy = vx + sh.R[0] * kTcSBP, *vz = vy + sh.R[1] * kTcSBP;
+    int *gi = reinterpret_cast<int *>(vz + sh.R[2] * kTcSBP);
+
+    // zero both operand buffers once: A rows >= P and B rows of absent coils stay zero
+    {
+        float4 *z = reinterpret_cast<float4 *>(smem);
+        const int n16 = (2 * sh.MT * kTcTileBytes + 2 * sh.N * kTcK * 4) / 16;
+        for (int e = tid; e < n16; e += kTcThreads) z[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(&tslot)),
+                     "r"(sh.ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mbar[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = tslot;
+    const uint32_t bar0 = tc_smem(&mbar[0]);  // mbarrier of buffer b at bar0 + 8 b
+    // instruction descriptor: D f32, A / B tf32, both K-major, N, M = 128
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(sh.N >> 3) << 17) | (8u << 24);
+
+    const int RXY = sh.R[0] * sh.R[1];
+    const int bc = tid >> 3, bs = tid & 7;  // B build: coil and sample of this thread (CC <= 32)
+    // A build: pairs e = tid + 256 j of (point p = e / 2, sample quad q = e % 2); per
+    // pair the byte offset of its 16-byte row slot in an A buffer and the shared
+    // addresses of its x / y / z weight-vector rows (+ 16 q bytes)
+    const uint32_t s0a = tc_smem(smem);
+    uint32_t pa[kTcPairs], px[kTcPairs], py[kTcPairs], pz[kTcPairs];
+#pragma unroll
+    for (int j = 0; j < kTcPairs; j++) {
+        const int e = tid + j * kTcThreads;
+        const int p = min(e >> 1, sh.P - 1), q = e & 1;
+        const int rz = p / RXY, rem = p - rz * RXY;
+        const int ry = rem / sh.R[0], rx = rem - ry * sh.R[0];
+        pa[j] = (uint32_t)((p >> 3) * kTcRowBytes + (p & 7) * 16 + q * 128);
+        px[j] = tc_smem(vx) + (uint32_t)(rx * kTcSBP + 4 * q) * 4;
+        py[j] = tc_smem(vy) + (uint32_t)(ry * kTcSBP + 4 * q) * 4;
+        pz[j] = tc_smem(vz) + (uint32_t)(rz * kTcSBP + 4 * q) * 4;
+    }
+    const int npairs = 2 * sh.P;
+    const uint64_t dbase = tc_desc(s0a);
+    uint32_t chunk_no = 0;  // chunks issued by this block (buffer = chunk_no & 1)
+    uint32_t uses0 = 0, uses1 = 0;  // commits issued per buffer
+
+    for (int task = blockIdx.x; task < nwork * nchunks; task += gridDim.x) {
+        const WorkItem it = work[task / nchunks];
+        const int64_t b0 = (int64_t)(task % nchunks) * sh.CC;
+        const int cact = (int)(batch - b0 < (int64_t)sh.CC ? batch - b0 : (int64_t)sh.CC);
+        const int f = it.bin / g.nbins;
+        int org[3];
+        {
+            const int lb = it.bin - f * g.nbins;
+            org[0] = (lb % g.nb[0]) * g.T[0];
+            org[1] = ((lb / g.nb[0]) % g.nb[1]) * g.T[1];
+            org[2] = (lb / (g.nb[0] * g.nb[1])) * g.T[2];
+        }
+        int first = 1;  // next MMA overwrites the accumulator
+        // k-space row and density-weight row of this thread's coil (B build)
+        const int64_t brow = (b0 + min(bc, max(cact - 1, 0))) * g.total;
+        const float2 *kc = reinterpret_cast<const float2 *>(ksp) + brow;
+        const float *kr = reinterpret_cast<const float *>(ksp) + brow;
+        const float *wrow = weight ? (wpb ? weight + brow : weight) : nullptr;
+        for (int base = it.begin; base < it.end; base += kTcSB) {
+            const int n = min(kTcSB, it.end - base);
+            __syncthreads();  // previous pass done with vx / vy / vz / gi
+            // stage per-axis weight vectors over the region (zero off the support)
+            for (int e = tid; e < 3 * kTcSB; e += kTcThreads) {
+                const int a = e / kTcSB, t = e - a * kTcSB;
+                float *v = a == 0 ? vx : (a == 1 ? vy : vz);
+                const int R = a == 0 ? sh.R[0] : (a == 1 ? sh.R[1] : sh.R[2]);
+                if (t < n) {
+                    const int j = base + t;
+                    const float k = a == 0 ? sc0[j] : (a == 1 ? sc1[j] : sc2[j]);
+                    const int G = a == 0 ? g.G[0] : (a == 1 ? g.G[1] : g.G[2]);
+                    const int oa = a == 0 ? org[0] : (a == 1 ? org[1] : org[2]);
+                    const double ihw = a == 0 ? g.inv_hw[0] : (a == 1 ? g.inv_hw[1] : g.inv_hw[2]);
+                    const float beta = a == 0 ? g.beta[0] : (a == 1 ? g.beta[1] : g.beta[2]);
+                    const int x0 = first_tap_dev(k, W);
+                    const int l = pmod(x0, G) - oa;  // in [0, T): the sample lies in this bin
+                    for (int r = 0; r < R; r++) v[r * kTcSBP + t] = 0.0f;
+                    if (l >= 0 && l + W <= R)
+                        for (int i = 0; i < W; i++) v[(l + i) * kTcSBP + t] = tap_weight(x0, i, k, W, ihw, beta);
+                    if (a == 0) gi[t] = sidx[j];
+                } else {
+                    for (int r = 0; r < R; r++) v[r * kTcSBP + t] = 0.0f;
+                    if (a == 0) gi[t] = -1;
+                }
+            }
+            __syncthreads();
+            const int nch = (n + kTcSC - 1) / kTcSC;
+            // coil-sample value of this thread for chunk ch of the pass (density-weighted)
+            // (the weight is applied at use: no wait on the loads here)
+            auto fetch = [&](int ch, float2 &v, float &wt) {
+                v = make_float2(0.0f, 0.0f);
+                wt = 1.0f;
+                if (ch < nch && bc < cact) {
+                    const int gidx = gi[ch * kTcSC + bs];
+                    if (gidx >= 0) {
+                        v = kreal ? make_float2(kr[gidx], 0.0f) : kc[gidx];
+                        if (wrow) wt = wrow[gidx];
+                    }
+                }
+            };
+            float2 pv0, pv1;
+            float pw0, pw1;
+            fetch(0, pv0, pw0);
+            fetch(1, pv1, pw1);
+            for (int ch = 0; ch < nch; ch++) {
+                const int buf = chunk_no & 1;
+                unsigned char *abuf = smem + buf * sh.MT * kTcTileBytes;
+                unsigned char *bbuf = bbase + buf * sh.N * (kTcK * 4);
+                const uint32_t bar = bar0 + 8 * buf;
+                const uint32_t nuse = buf ? uses1 : uses0;
+                if (chunk_no >= 2) {
+                    // the MMAs of chunk chunk_no - 2 read this buffer
+                    if (!tc_wait(bar, nuse - 1)) s_abort = 1;
+                }
+                const int s0 = ch * kTcSC;
+                // A: thread per (point, sample quad), addresses precomputed
+                {
+                    const uint32_t ab = tc_smem(abuf), vo = (uint32_t)s0 * 4;
+#pragma unroll
+                    for (int j = 0; j < kTcPairs; j++) {
+                        if (tid + j * kTcThreads >= npairs) break;
+                        const float4 x = tc_lds4(px[j] + vo);
+                        const float4 y = tc_lds4(py[j] + vo);
+                        const float4 z = tc_lds4(pz[j] + vo);
+                        const float4 w =
+                            make_float4(x.x * y.x * z.x, x.y * y.y * z.y, x.z * y.z * z.z, x.w * y.w * z.w);
+                        const float4 h = make_float4(tc_hi(w.x), tc_hi(w.y), tc_hi(w.z), tc_hi(w.w));
+                        tc_sts4(ab + pa[j], h);
+                        tc_sts4(ab + pa[j] + 256, make_float4(w.x - h.x, w.y - h.y, w.z - h.z, w.w - h.w));
+                    }
+                }
+                // B: thread (coil c, sample s) of the chunk; absent coils / samples are zeros
+                if (tid < sh.CC * kTcSC) {
+                    const float2 v = make_float2(pv0.x * pw0, pv0.y * pw0);
+                    const float hx = tc_hi(v.x), hy = tc_hi(v.y);
+                    // rows 2c (real) and 2c + 1 (imaginary); K: hi at s, lo at 8 + s
+                    unsigned char *r0 = bbuf + ((2 * bc) >> 3) * kTcRowBytes + ((2 * bc) & 7) * 16;
+                    unsigned char *r1 = r0 + 16;
+                    const int ko = (bs >> 2) * 128 + (bs & 3) * 4;
+                    *reinterpret_cast<float *>(r0 + ko) = hx;
+                    *reinterpret_cast<float *>(r0 + ko + 256) = v.x - hx;
+                    *reinterpret_cast<float *>(r1 + ko) = hy;
+                    *reinterpret_cast<float *>(r1 + ko + 256) = v.y - hy;
+                }
+                // values of chunk ch + 2 are loaded two chunks ahead of their use
+                pv0 = pv1;
+                pw0 = pw1;
+                fetch(ch + 2, pv1, pw1);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (s_abort) goto done;
+                if (tid == 0) {
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    // descriptors differ from the one of the smem base only in the start address
+                    const uint64_t da0 = dbase + ((tc_smem(abuf) - s0a) >> 4), db0 = dbase + ((tc_smem(bbuf) - s0a) >> 4);
+                    for (int mt = 0; mt < sh.MT; mt++)
+#pragma unroll
+                        for (int ks = 0; ks < 3; ks++) {
+                            // hi*hi, hi*lo, lo*hi: K blocks at byte 0 (hi) and 256 (lo)
+                            const uint64_t da = da0 + ((mt * kTcTileBytes + (ks == 2 ? 256 : 0)) >> 4);
+                            const uint64_t db = db0 + (ks == 1 ? 16 : 0);
+                            const uint32_t acc = (first && ks == 0) ? 0u : 1u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                                    tbase + (uint32_t)(mt * sh.N)),
+                                "l"(da), "l"(db), "r"(idesc), "r"(acc));
+                        }
+                    asm volatile(
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                        : "memory");
+                }
+                first = 0;
+                if (buf) uses1++; else uses0++;
+                chunk_no++;
+            }
+        }
+        if (first) continue;  // no samples (cannot happen for a planned item)
+        // epilogue: wait for the last chunk, read the accumulators, add to the grid
+        {
+            const int lb = (chunk_no - 1) & 1;
+            if (!tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1)) s_abort = 1;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (s_abort) goto done;
+        if (warp < 8) {
+            const int quarter = warp & 3, half = warp >> 2;
+            const int ncol = sh.N / 2;  // columns of this warp (its half of the coils)
+            for (int mt = 0; mt < sh.MT; mt++) {
+                const int p = mt * 128 + quarter * 32 + lane;
+                int64_t gp = -1;
+                if (p < sh.P) {
+                    const int rz = p / RXY, rem = p - rz * RXY;
+                    const int ry = rem / sh.R[0], rx = rem - ry * sh.R[0];
+                    const int px = (org[0] + rx + g.G[0] - g.half[0]) % g.G[0];
+                    const int py = (org[1] + ry + g.G[1] - g.half[1]) % g.G[1];
+                    const int pz = (org[2] + rz + g.G[2] - g.half[2]) % g.G[2];
+                    gp = ((int64_t)pz * g.G[1] + py) * g.G[0] + px;
+                }
+                for (int c0 = half * ncol; c0 < (half + 1) * ncol; c0 += 16) {
+                    uint32_t r[16];
+                    tc_ld16(tbase + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(mt * sh.N + c0), r);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    if (gp >= 0) {
+#pragma unroll
+                        for (int i = 0; i < 8; i++) {
+                            const int c = c0 / 2 + i;
+                            const float2 v = make_float2(__uint_as_float(r[2 * i]) * inv_scale,
+                                                         __uint_as_float(r[2 * i + 1]) * inv_scale);
+                            if (c < cact && (v.x != 0.0f || v.y != 0.0f))
+                                atomicAdd(grid + ((b0 + c) * g.nframes + f) * g.gsize + gp, v);
+                        }
+                    }
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        // the next task's first MMAs overwrite the accumulator after its build barrier
+    }
+done:
+    if (s_abort && tid == 0) atomicAdd(&g_tc_timeouts, 1);
+    // let the last commit land before the tensor memory is released (bounded)
+    if (tid == 0 && chunk_no > 0) {
+        const int lb = (chunk_no - 1) & 1;
+        tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(sh.ncols));
+}
+
+static int tc_disabled()
+{
+    static const int v = [] {
+        const char *e = getenv("DMR_NO_TC");
+        return e && atoi(e) ? 1 : 0;
+    }();
+    return v;
+}
+
+static bool tc_shape(const Geom &g, int64_t batch, TcShape &s)
+{
+    if (g.ndim != 3 || batch < 1) return false;
+    const int W = g.W[0];
+    if (W < 2 || g.W[1] != W || g.W[2] != W) return false;
+    for (int a = 0; a < 3; a++) s.R[a] = g.T[a] + W - 1;
+    s.P = s.R[0] * s.R[1] * s.R[2];
+    if (s.P > kTcMaxMT * 128 || s.R[0] + s.R[1] + s.R[2] > 64) return false;
+    s.MT = (s.P + 127) / 128;
+    s.CC = (int)std::min<int64_t>(batch, kTcMaxCC);
+    s.N = std::max(32, (2 * s.CC + 31) / 32 * 32);  // two warps split a tile's columns in 16s
+    const int need = s.MT * s.N;
+    s.ncols = 32;
+    while (s.ncols < need) s.ncols <<= 1;
+    return s.ncols <= 512;
+}
+
+// Tensor-core gridding of a 3D plan (atomic accumulation); DMR_ERR_UNSUPPORTED
+// when the geometry does not fit (then the caller uses the cell-cube kernels).
+int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                     const float *weight, int wpb, cudaStream_t st)
+{
+    TcShape sh;
+    if (tc_disabled() || !tc_shape(p->g, batch, sh)) return DMR_ERR_UNSUPPORTED;
+    int dev = 0, sms = 0, smem_sm = 0, smem_blk = 0;
+    DMR_CUDA(cudaGetDevice(&dev));
+    DMR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DMR_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    DMR_CUDA(cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    size_t smem = tc_smem_bytes(sh);
+    // resident blocks of one SM must not ask for more than its 512 tensor-memory
+    // columns: pad the shared memory so that at most 512 / ncols blocks fit
+    const int maxb = 512 / sh.ncols;
+    const size_t reserve = 2048 + 64;  // per-block driver reserve + static shared memory
+    if ((size_t)smem_sm / (smem + reserve) > (size_t)maxb) smem = (size_t)smem_sm / (maxb + 1) - reserve + 16;
+    if (smem > (size_t)smem_blk) return DMR_ERR_UNSUPPORTED;
+    const int per_sm = std::max(1, std::min(maxb, (int)((size_t)smem_sm / (smem + reserve))));
+    DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
+    if (p->nwork == 0) return DMR_OK;
+    const int64_t nchunks = ceil_div(batch, sh.CC);
+    const int64_t tasks = (int64_t)p->nwork * nchunks;
+    DMR_CHECK(tasks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
+    const int blocks = (int)std::min<int64_t>(tasks, (int64_t)sms * per_sm);
+    DMR_CUDA(cudaFuncSetAttribute(grid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    grid_tc_kernel<<<blocks, kTcThreads, smem, st>>>(p->g, sh, p->work, p->nwork, (int)nchunks, p->scoord[0],
+                                                      p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid,
+                                                      batch, weight, wpb, (float)(1.0 / p->scale));
+    DMR_LAUNCHED("grid_tc_kernel");
+    return DMR_OK;
+}
+
+}  // namespace dmr

@@ -1,0 +1,109 @@
+"""GPU parity of the tensor-core 3D gridding (atomic mode, tcgen05 TF32 with a
+three-term split) against the oracle and against the deterministic gridding
+kernels, which share no code with it.
+
+Cases: coil counts below, at and above the 32 coils of one block (a partial
+last coil chunk), one and several frames, real input, shared and per-batch
+density weights, kernel widths 3..5 (bin regions of 216..512 points) and
+width 6 at oversampling 2 (a larger region: the cell-cube kernels run). Tolerance: relative L2 error
+<= 1e-5 in float32.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def rel(a, b):
+    a = np.asarray(a.detach().cpu() if isinstance(a, torch.Tensor) else a, dtype=np.complex128)
+    b = np.asarray(b.detach().cpu() if isinstance(b, torch.Tensor) else b, dtype=np.complex128)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+@pytest.fixture(scope="module")
+def F():
+    import deepmr_b200.fft as F
+
+    return F
+
+
+def _grid(F, plan, ksp, weight=None, det=False):
+    old = F.set_deterministic_gridding(det)
+    try:
+        return F.apply_nufft_adj(ksp, plan, weight=weight)
+    finally:
+        F.set_deterministic_gridding(old)
+
+
+@pytest.mark.parametrize("ncoils", [1, 5, 32, 40])
+def test_tc_grid_vs_oracle(F, ncoils):
+    from oracle import nufft_ref as R
+    from deepmr_b200 import synth
+
+    n = 20
+    coord = synth.kooshball_3d(300, 2 * n, n).astype(np.float32)
+    c = torch.as_tensor(coord)
+    plan = F.plan_nufft(c, n, 4, 1.25, device="cuda")
+    ksp = synth.complex_gaussian((ncoils,) + coord.shape[:-1], seed=ncoils)
+    dcf = torch.as_tensor(synth.ramp_dcf(coord.reshape(-1, 3)).reshape(coord.shape[:-1]))
+    x = _grid(F, plan, ksp.cuda(), dcf.cuda())
+    ref = R.apply_nufft_adj(ksp, R.plan_nufft(c, n, 4, 1.25), weight=dcf)
+    assert rel(x, ref) < TOL
+
+
+@pytest.mark.parametrize("width,os", [(3, 1.25), (4, 1.25), (5, 1.25), (6, 2.0)])
+def test_tc_grid_widths_vs_oracle(F, width, os):
+    from oracle import nufft_ref as R
+    from deepmr_b200 import synth
+
+    n = 20
+    coord = synth.kooshball_3d(300, 2 * n, n).astype(np.float32)
+    c = torch.as_tensor(coord)
+    plan = F.plan_nufft(c, n, width, os, device="cuda")
+    ksp = synth.complex_gaussian((6,) + coord.shape[:-1], seed=width)
+    ref = R.apply_nufft_adj(ksp, R.plan_nufft(c, n, width, os))
+    assert rel(_grid(F, plan, ksp.cuda()), ref) < TOL
+
+
+def test_tc_grid_vs_deterministic(F):
+    from deepmr_b200 import synth
+
+    n = 32
+    coord = synth.kooshball_3d(1200, 2 * n, n).astype(np.float32)
+    plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
+    ksp = synth.complex_gaussian((12,) + coord.shape[:-1], seed=4).cuda()
+    assert rel(_grid(F, plan, ksp), _grid(F, plan, ksp, det=True)) < TOL
+
+
+def test_tc_grid_frames_real_batch_weights(F):
+    from deepmr_b200 import synth
+
+    n, nf = 24, 3
+    coord = np.stack([synth.kooshball_3d(400, 2 * n, n) * (1.0 - 0.07 * f) for f in range(nf)]).astype(np.float32)
+    plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
+    ksp = synth.complex_gaussian((2, 17, nf) + coord.shape[1:-1], seed=3).real.contiguous().cuda()
+    wb = torch.rand((2, 17, nf) + coord.shape[1:-1], generator=torch.Generator().manual_seed(4)).cuda()
+    x = _grid(F, plan, ksp, wb)
+    assert tuple(x.shape) == (2, 17, nf, n, n, n)
+    assert rel(x, _grid(F, plan, ksp, wb, det=True)) < TOL
+
+
+def test_tc_grid_adjoint_identity(F):
+    """<A x, y> = G <x, A^H y> with the tensor-core adjoint."""
+    from deepmr_b200 import synth
+
+    n = 24
+    coord = synth.kooshball_3d(600, 2 * n, n).astype(np.float32)
+    plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
+    x = synth.complex_gaussian((8, n, n, n), seed=5).cuda()
+    y = synth.complex_gaussian((8,) + coord.shape[:-1], seed=6).cuda()
+    ax = F.apply_nufft(x, plan)
+    ahy = _grid(F, plan, y)
+    G = float(np.prod([int(s) for s in plan.os_shape]))
+    lhs = torch.vdot(ax.flatten().to(torch.complex128), y.flatten().to(torch.complex128))
+    rhs = G * torch.vdot(x.flatten().to(torch.complex128), ahy.flatten().to(torch.complex128))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
