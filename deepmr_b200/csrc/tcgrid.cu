@@ -44,7 +44,7 @@
 
 namespace dmr {
 
-constexpr int kTcThreads = 384;       // 12 warps; warps 0-7 read the accumulator (two per lane quarter)
+constexpr int kTcThreads = 384;       // 12 warps (384: 20.0 ms vs 21.2 with 512 and 23.2 with 256, 192^3 kooshball)
 constexpr int kTcSC = 8;              // samples per MMA chunk
 constexpr int kTcK = 2 * kTcSC;       // K extent of a chunk in shared memory ([hi | lo])
 constexpr int kTcSB = 128;            // samples staged per pass
@@ -202,8 +202,34 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
     uint32_t chunk_no = 0;  // chunks issued by this block (buffer = chunk_no & 1)
     uint32_t uses0 = 0, uses1 = 0;  // commits issued per buffer
 
-    for (int task = blockIdx.x; task < nwork * nchunks; task += gridDim.x) {
-        const WorkItem it = work[task / nchunks];
+    // staging role of this thread: axis sa of sample st of a pass (384 = 3 x 128)
+    static_assert(kTcThreads == 3 * kTcSB, "one (axis, sample) per thread in the staging");
+    const int sa = tid / kTcSB, st = tid - sa * kTcSB;
+    const float *ssc = sa == 0 ? sc0 : (sa == 1 ? sc1 : sc2);
+    float *sv = sa == 0 ? vx : (sa == 1 ? vy : vz);
+    const int sR = sa == 0 ? sh.R[0] : (sa == 1 ? sh.R[1] : sh.R[2]);
+    const int sG = sa == 0 ? g.G[0] : (sa == 1 ? g.G[1] : g.G[2]);
+    const double sihw = sa == 0 ? g.inv_hw[0] : (sa == 1 ? g.inv_hw[1] : g.inv_hw[2]);
+    const float sbeta = sa == 0 ? g.beta[0] : (sa == 1 ? g.beta[1] : g.beta[2]);
+    // inputs of the first pass of the next task, loaded while the current one runs
+    const int ntasks = nwork * nchunks;
+    WorkItem nxt = {0, 0, 0};
+    float pk = 0.0f;
+    int psid = -1;
+    if (blockIdx.x < ntasks) {
+        nxt = work[blockIdx.x / nchunks];
+        if (st < nxt.end - nxt.begin) {
+            pk = ssc[nxt.begin + st];
+            psid = sa == 0 ? sidx[nxt.begin + st] : 0;
+        }
+    }
+
+    for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+        const WorkItem it = nxt;
+        const float k_first = pk;
+        const int sid_first = psid;
+        const int ntask = task + gridDim.x;
+        if (ntask < ntasks) nxt = work[ntask / nchunks];
         const int64_t b0 = (int64_t)(task % nchunks) * sh.CC;
         const int cact = (int)(batch - b0 < (int64_t)sh.CC ? batch - b0 : (int64_t)sh.CC);
         const int f = it.bin / g.nbins;
@@ -214,6 +240,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
             org[1] = ((lb / g.nb[0]) % g.nb[1]) * g.T[1];
             org[2] = (lb / (g.nb[0] * g.nb[1])) * g.T[2];
         }
+        const int soa = sa == 0 ? org[0] : (sa == 1 ? org[1] : org[2]);
         int first = 1;  // next MMA overwrites the accumulator
         // k-space row and density-weight row of this thread's coil (B build)
         const int64_t brow = (b0 + min(bc, max(cact - 1, 0))) * g.total;
@@ -224,27 +251,23 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
             const int n = min(kTcSB, it.end - base);
             __syncthreads();  // previous pass done with vx / vy / vz / gi
             // stage per-axis weight vectors over the region (zero off the support)
-            for (int e = tid; e < 3 * kTcSB; e += kTcThreads) {
-                const int a = e / kTcSB, t = e - a * kTcSB;
-                float *v = a == 0 ? vx : (a == 1 ? vy : vz);
-                const int R = a == 0 ? sh.R[0] : (a == 1 ? sh.R[1] : sh.R[2]);
-                if (t < n) {
-                    const int j = base + t;
-                    const float k = a == 0 ? sc0[j] : (a == 1 ? sc1[j] : sc2[j]);
-                    const int G = a == 0 ? g.G[0] : (a == 1 ? g.G[1] : g.G[2]);
-                    const int oa = a == 0 ? org[0] : (a == 1 ? org[1] : org[2]);
-                    const double ihw = a == 0 ? g.inv_hw[0] : (a == 1 ? g.inv_hw[1] : g.inv_hw[2]);
-                    const float beta = a == 0 ? g.beta[0] : (a == 1 ? g.beta[1] : g.beta[2]);
+            {
+                for (int r = 0; r < sR; r++) sv[r * kTcSBP + st] = 0.0f;
+                int sid = -1;
+                if (st < n) {
+                    const float k = base == it.begin ? k_first : ssc[base + st];
+                    sid = sa == 0 ? (base == it.begin ? sid_first : sidx[base + st]) : 0;
                     const int x0 = first_tap_dev(k, W);
-                    const int l = pmod(x0, G) - oa;  // in [0, T): the sample lies in this bin
-                    for (int r = 0; r < R; r++) v[r * kTcSBP + t] = 0.0f;
-                    if (l >= 0 && l + W <= R)
-                        for (int i = 0; i < W; i++) v[(l + i) * kTcSBP + t] = tap_weight(x0, i, k, W, ihw, beta);
-                    if (a == 0) gi[t] = sidx[j];
-                } else {
-                    for (int r = 0; r < R; r++) v[r * kTcSBP + t] = 0.0f;
-                    if (a == 0) gi[t] = -1;
+                    const int l = pmod(x0, sG) - soa;  // in [0, T): the sample lies in this bin
+                    if (l >= 0 && l + W <= sR)
+                        for (int i = 0; i < W; i++) sv[(l + i) * kTcSBP + st] = tap_weight(x0, i, k, W, sihw, sbeta);
                 }
+                if (sa == 0) gi[st] = sid;
+            }
+            // last pass of the task: fetch the next task's first-pass inputs now
+            if (base + kTcSB >= it.end && ntask < ntasks && st < nxt.end - nxt.begin) {
+                pk = ssc[nxt.begin + st];
+                psid = sa == 0 ? sidx[nxt.begin + st] : 0;
             }
             __syncthreads();
             const int nch = (n + kTcSC - 1) / kTcSC;
@@ -347,9 +370,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         __syncthreads();
         if (s_abort) goto done;
-        if (warp < 8) {
+        // warps (quarter, part): the accumulator columns split in nparts ranges of 16+
+        int nparts = min(kTcThreads / 128, sh.N / 16);
+        while ((sh.N / 16) % nparts) nparts--;
+        if ((warp >> 2) < nparts) {
             const int quarter = warp & 3, half = warp >> 2;
-            const int ncol = sh.N / 2;  // columns of this warp (its half of the coils)
+            const int ncol = sh.N / nparts;  // columns of this warp
             for (int mt = 0; mt < sh.MT; mt++) {
                 const int p = mt * 128 + quarter * 32 + lane;
                 int64_t gp = -1;
