@@ -487,6 +487,27 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
         DMR_CUDA(cudaMemcpyAsync(p->det_work, det.data(), det.size() * sizeof(WorkItem),
                                  cudaMemcpyHostToDevice, st));
 
+    // the same items visited in 4x4x4-bin tiles (frame, tile z, y, x, bin z, y, x):
+    // bins that share halo points or spokes run close together, so their grid
+    // lines and k-space sectors are still in L2 (DMR_NO_TILED_ORDER=1: key order)
+    std::vector<int32_t> worder(items.size());
+    for (size_t i = 0; i < items.size(); i++) worder[i] = (int32_t)i;
+    static const bool tiled_order = [] {
+        const char *e = getenv("DMR_NO_TILED_ORDER");
+        return !(e && atoi(e));
+    }();
+    if (tiled_order) {
+        auto tkey = [&](const WorkItem &w) {
+            const int64_t f = w.bin / g.nbins, lb = w.bin % g.nbins;
+            const int64_t bx = lb % g.nb[0], by = (lb / g.nb[0]) % g.nb[1], bz = lb / ((int64_t)g.nb[0] * g.nb[1]);
+            const int64_t tx = bx >> 2, ty = by >> 2, tz = bz >> 2;
+            const int64_t ntx = (g.nb[0] + 3) >> 2, nty = (g.nb[1] + 3) >> 2, ntz = (g.nb[2] + 3) >> 2;
+            const int64_t tile = ((f * ntz + tz) * nty + ty) * ntx + tx;
+            return tile * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3));
+        };
+        std::stable_sort(worder.begin(), worder.end(),
+                         [&](int32_t a, int32_t b) { return tkey(items[a]) < tkey(items[b]); });
+    }
     p->nwork = (int)items.size();
     p->ntiles = (int)order.size();
     DMR_TRY(dev_alloc(&p->bin_start, nkeys + 1));
@@ -494,9 +515,13 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     DMR_TRY(dev_alloc(&p->tiles, order.size()));
     DMR_CUDA(cudaMemcpyAsync(p->bin_start, h_start.data(), (nkeys + 1) * sizeof(int32_t),
                              cudaMemcpyHostToDevice, st));
-    if (!items.empty())
+    DMR_TRY(dev_alloc(&p->work_order, items.size()));
+    if (!items.empty()) {
         DMR_CUDA(cudaMemcpyAsync(p->work, items.data(), items.size() * sizeof(WorkItem),
                                  cudaMemcpyHostToDevice, st));
+        DMR_CUDA(cudaMemcpyAsync(p->work_order, worder.data(), worder.size() * sizeof(int32_t),
+                                 cudaMemcpyHostToDevice, st));
+    }
     DMR_CUDA(cudaMemcpyAsync(p->tiles, order.data(), order.size() * sizeof(int32_t),
                              cudaMemcpyHostToDevice, st));
     DMR_CUDA(cudaStreamSynchronize(st));

@@ -88,6 +88,7 @@ struct dmr_plan {
     int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
     dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
     int nwork = 0;
+    int32_t *work_order = nullptr;      // item order in 4x4x4-bin tiles (L2 reuse of halos and spokes)
     int32_t *tiles = nullptr;           // owner-gridding tile order (heavy first)
     int ntiles = 0;
     // deterministic gridding: whole non-empty bins grouped by colour; bins of
@@ -113,6 +114,7 @@ struct dmr_plan {
         cudaFree(sidx);
         cudaFree(bin_start);
         cudaFree(work);
+        cudaFree(work_order);
         cudaFree(tiles);
         cudaFree(det_work);
         cudaFree(foff_dev);

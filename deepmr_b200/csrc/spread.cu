@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     constexpr int NG = S::NG, SPL = S::SPL, INS = S::INS, NW = S::NW;
     extern __shared__ __align__(16) unsigned char smem[];
     const int CC = 1 << cc_log2;
-    const WorkItem it = work[blockIdx.x];
+    const WorkItem it = work[blockIdx.x];  // key order (16.2 vs 15.7 ms in 4x4x4-bin tiles)
     const int f = it.bin / g.nbins;
     int org[3];
     tile_origin(g, it.bin - f * g.nbins, org);

@@ -136,7 +136,7 @@ __host__ __device__ inline size_t tc_smem_bytes(const TcShape &s)
 }
 
 __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
-    Geom g, TcShape sh, const WorkItem *__restrict__ work, int nwork, int nchunks,
+    Geom g, TcShape sh, const WorkItem *__restrict__ work, const int32_t *__restrict__ order, int nwork, int nchunks,
     const float *__restrict__ sc0, const float *__restrict__ sc1, const float *__restrict__ sc2,
     const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid,
     int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale)
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
     float pk = 0.0f;
     int psid = -1;
     if (blockIdx.x < ntasks) {
-        nxt = work[blockIdx.x / nchunks];
+        nxt = work[order[blockIdx.x / nchunks]];
         if (st < nxt.end - nxt.begin) {
             pk = ssc[nxt.begin + st];
             psid = sa == 0 ? sidx[nxt.begin + st] : 0;
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
         const float k_first = pk;
         const int sid_first = psid;
         const int ntask = task + gridDim.x;
-        if (ntask < ntasks) nxt = work[ntask / nchunks];
+        if (ntask < ntasks) nxt = work[order[ntask / nchunks]];
         const int64_t b0 = (int64_t)(task % nchunks) * sh.CC;
         const int cact = (int)(batch - b0 < (int64_t)sh.CC ? batch - b0 : (int64_t)sh.CC);
         const int f = it.bin / g.nbins;
@@ -473,7 +473,7 @@ int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     DMR_CHECK(tasks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
     const int blocks = (int)std::min<int64_t>(tasks, (int64_t)sms * per_sm);
     DMR_CUDA(cudaFuncSetAttribute(grid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    grid_tc_kernel<<<blocks, kTcThreads, smem, st>>>(p->g, sh, p->work, p->nwork, (int)nchunks, p->scoord[0],
+    grid_tc_kernel<<<blocks, kTcThreads, smem, st>>>(p->g, sh, p->work, p->work_order, p->nwork, (int)nchunks, p->scoord[0],
                                                       p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid,
                                                       batch, weight, wpb, (float)(1.0 / p->scale));
     DMR_LAUNCHED("grid_tc_kernel");
