@@ -447,13 +447,14 @@ def _pipelinable(host, dev, batch, out_item_bytes):
     return nbytes >= PIPELINE_MIN_BYTES
 
 
-def _pipelined(x_h, out_h, batch, dev, run, ws_bytes):
+def _pipelined(x_h, out_h, batch, dev, run, ws_bytes, min_chunk=1):
     """Run ``run(x_dev, out_dev, b0, nb, ws, stream)`` over chunks of the
     flattened batch: ``x_h`` (batch, ...) and ``out_h`` (batch, ...) are pinned
     host tensors, device input/output buffers are double-buffered, and the
     compute stream runs the chunks in order with one workspace. Returns after
-    every copy out has completed (``out_h`` is then valid on the host)."""
-    nch = min(batch, PIPELINE_CHUNKS)
+    every copy out has completed (``out_h`` is then valid on the host).
+    Chunks hold at least ``min_chunk`` batch items."""
+    nch = max(1, min(PIPELINE_CHUNKS, batch // max(1, min_chunk)))
     cb = -(-batch // nch)
     nch = -(-batch // cb)
     h2d, comp, d2h = _pipe_streams(dev)
@@ -582,11 +583,15 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
             )
         )
 
-    if _pipelinable(kspace, dev, batch, 8 * int(np.prod(item))):
+    # the 3D tensor-core gridding costs about the same for 8 coils as for 32
+    # (the spreading weights are built once per sample and launch), so the
+    # adjoint's chunks keep at least 8 batch items
+    min_chunk = 8 if nufft_plan.ndim == 3 else 1
+    if batch >= 2 * min_chunk and _pipelinable(kspace, dev, batch, 8 * int(np.prod(item))):
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
         out = torch.empty([batch] + item, dtype=torch.complex64, pin_memory=True)
         _pipelined(kspace.reshape((batch,) + tuple(kspace.shape[len(batch_shape):])), out, batch, dev, run,
-                   interp.workspace)
+                   interp.workspace, min_chunk)
         return out.reshape(list(batch_shape) + item)
     y = kspace.to(dev).contiguous()
     out = torch.empty(list(batch_shape) + item, dtype=torch.complex64, device=dev)

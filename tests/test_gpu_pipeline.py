@@ -40,9 +40,9 @@ def spy(F, monkeypatch):
     calls = []
     orig = N._pipelined
 
-    def wrapped(x_h, out_h, batch, dev, run, ws_bytes):
+    def wrapped(x_h, out_h, batch, dev, run, ws_bytes, *rest):
         calls.append(batch)
-        return orig(x_h, out_h, batch, dev, run, ws_bytes)
+        return orig(x_h, out_h, batch, dev, run, ws_bytes, *rest)
 
     monkeypatch.setattr(N, "PIPELINE_MIN_BYTES", 0)
     monkeypatch.setattr(N, "_pipelined", wrapped)
@@ -114,14 +114,15 @@ def test_pipeline_not_taken_for_pageable_or_single(F, spy):
 
 
 def test_pipeline_default_threshold_3d(F):
-    """A 3D 8-coil call above the default size runs chunked and matches."""
+    """3D calls above the default size run chunked (the adjoint in chunks of at
+    least 8 coils) and match the device-input calls."""
     from deepmr_b200 import synth
     N = importlib.import_module("deepmr_b200.fft.nufft")
 
     n = 64
     coord = synth.kooshball_3d(8192, 2 * n, n).astype(np.float32)
     plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
-    ksp = synth.complex_gaussian((8,) + coord.shape[:-1], seed=5)
+    ksp = synth.complex_gaussian((16,) + coord.shape[:-1], seed=5)
     assert ksp.numel() * 8 >= N.PIPELINE_MIN_BYTES
     x_h = F.apply_nufft_adj(ksp.pin_memory(), plan)
     x_d = F.apply_nufft_adj(ksp.cuda(), plan)
