@@ -30,6 +30,7 @@ SYMBOLS = (
     "dmr_version",
     "dmr_last_error",
     "dmr_launch_count",
+    "dmr_tc_timeouts",
     "dmr_detect_cartesian",
     "dmr_plan_create",
     "dmr_plan_destroy",
@@ -79,6 +80,7 @@ _SIGS = {
     "dmr_version": (ctypes.c_int, []),
     "dmr_last_error": (ctypes.c_char_p, []),
     "dmr_launch_count": (i64, []),
+    "dmr_tc_timeouts": (ctypes.c_int, [i64p, ctypes.c_int]),
     "dmr_detect_cartesian": (ctypes.c_int, [vp, i64, ctypes.c_int, i32p, i32p, vp]),
     "dmr_plan_create": (
         ctypes.c_int,

@@ -481,3 +481,19 @@ int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
 }
 
 }  // namespace dmr
+
+using namespace dmr;
+
+extern "C" int dmr_tc_timeouts(int64_t *count, int reset)
+{
+    DMR_CHECK(count, DMR_ERR_INVALID, "count is NULL");
+    int v = 0;
+    DMR_CUDA(cudaDeviceSynchronize());
+    DMR_CUDA(cudaMemcpyFromSymbol(&v, g_tc_timeouts, sizeof(int)));
+    *count = v;
+    if (reset) {
+        const int zero = 0;
+        DMR_CUDA(cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)));
+    }
+    return DMR_OK;
+}

@@ -57,6 +57,14 @@ const char *dmr_last_error(void);
 int64_t dmr_launch_count(void);
 
 /*
+ * Bounded waits of the tensor-core gridding kernel that ran out on the current
+ * device since load (each such block stops issuing work and frees its tensor
+ * memory; the count should stay 0). Reads after a device synchronisation;
+ * reset != 0 zeroes the counter. No reference counterpart (device health).
+ */
+int dmr_tc_timeouts(int64_t *count, int reset);
+
+/*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
  * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
  * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the

@@ -107,3 +107,18 @@ def test_tc_grid_adjoint_identity(F):
     lhs = torch.vdot(ax.flatten().to(torch.complex128), y.flatten().to(torch.complex128))
     rhs = G * torch.vdot(x.flatten().to(torch.complex128), ahy.flatten().to(torch.complex128))
     assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_tc_grid_no_wait_ran_out(F):
+    """The kernel's bounded mbarrier waits never ran out during these tests."""
+    import ctypes
+
+    from deepmr_b200 import _lib, synth
+
+    n = 16
+    coord = synth.kooshball_3d(200, 2 * n, n).astype(np.float32)
+    plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
+    _grid(F, plan, synth.complex_gaussian((4,) + coord.shape[:-1], seed=7).cuda())
+    count = ctypes.c_int64(-1)
+    _lib.check(_lib.lib().dmr_tc_timeouts(ctypes.byref(count), 0))
+    assert count.value == 0
