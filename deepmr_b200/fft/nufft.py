@@ -447,6 +447,14 @@ def _pipelinable(host, dev, batch, out_item_bytes):
     return nbytes >= PIPELINE_MIN_BYTES
 
 
+def _pipeline_chunks(batch, min_chunk=1):
+    """(number of chunks, batch items per chunk) of the host pipeline: up to
+    PIPELINE_CHUNKS chunks of at least ``min_chunk`` items, equal but the last."""
+    nch = max(1, min(PIPELINE_CHUNKS, batch // max(1, min_chunk)))
+    cb = -(-batch // nch)
+    return -(-batch // cb), cb
+
+
 def _pipelined(x_h, out_h, batch, dev, run, ws_bytes, min_chunk=1):
     """Run ``run(x_dev, out_dev, b0, nb, ws, stream)`` over chunks of the
     flattened batch: ``x_h`` (batch, ...) and ``out_h`` (batch, ...) are pinned
@@ -454,9 +462,7 @@ def _pipelined(x_h, out_h, batch, dev, run, ws_bytes, min_chunk=1):
     compute stream runs the chunks in order with one workspace. Returns after
     every copy out has completed (``out_h`` is then valid on the host).
     Chunks hold at least ``min_chunk`` batch items."""
-    nch = max(1, min(PIPELINE_CHUNKS, batch // max(1, min_chunk)))
-    cb = -(-batch // nch)
-    nch = -(-batch // cb)
+    nch, cb = _pipeline_chunks(batch, min_chunk)
     h2d, comp, d2h = _pipe_streams(dev)
     with torch.cuda.device(dev):
         cur = torch.cuda.current_stream(dev)
