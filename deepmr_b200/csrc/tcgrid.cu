@@ -463,7 +463,10 @@ int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     // columns: pad the shared memory so that at most 512 / ncols blocks fit
     const int maxb = 512 / sh.ncols;
     const size_t reserve = 2048 + 64;  // per-block driver reserve + static shared memory
-    if ((size_t)smem_sm / (smem + reserve) > (size_t)maxb) smem = (size_t)smem_sm / (maxb + 1) - reserve + 16;
+    // (padded with 1 KB to spare, so maxb + 1 blocks cannot fit whatever the
+    // allocation granularity; a block that found no free columns would wait in
+    // tcgen05.alloc until a co-resident block exits)
+    if ((size_t)smem_sm / (smem + reserve) > (size_t)maxb) smem = (size_t)smem_sm / (maxb + 1) - 1024;
     if (smem > (size_t)smem_blk) return DMR_ERR_UNSUPPORTED;
     const int per_sm = std::max(1, std::min(maxb, (int)((size_t)smem_sm / (smem + reserve))));
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
