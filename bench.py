@@ -219,9 +219,46 @@ class CpuBaseline:
                            f"(oracle: C loops with OpenMP + torch CPU FFT, {self.cores} threads)")
 
 
+def parity_check(F, cb, plan, img, ksp, dcf, coils=(0, 1)):
+    """Relative L2 error of the timed GPU path against the oracle at the full
+    workload size, on two of its coils (coils are independent): forward,
+    atomic (tensor-core) adjoint and deterministic adjoint."""
+    R, sel = cb.R, list(coils)
+
+    def rel(a, b):
+        a = np.asarray(torch.as_tensor(a).cpu(), dtype=np.complex128).ravel()
+        b = np.asarray(torch.as_tensor(b).cpu(), dtype=np.complex128).ravel()
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    out = {"tol": 1e-5, "coils": sel, "reference": "oracle (CPU restatement of the reference), same inputs"}
+    out["forward_rel_l2"] = rel(F.apply_nufft(img, plan)[sel], R.apply_nufft(img[sel].cpu(), cb.plan))
+    x_ref = R.apply_nufft_adj(ksp[sel].cpu(), cb.plan, weight=dcf.cpu())
+    for name, det in (("adjoint_atomic_rel_l2", False), ("adjoint_deterministic_rel_l2", True)):
+        old = F.set_deterministic_gridding(det)
+        try:
+            x = F.apply_nufft_adj(ksp, plan, weight=dcf)[sel]
+            plan.interpolator.check_status()
+        finally:
+            F.set_deterministic_gridding(old)
+        out[name] = rel(x, x_ref)
+    out["pass"] = all(v < out["tol"] for k, v in out.items() if k.endswith("_rel_l2"))
+    return out
+
+
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def bench_config(w, args, world, deterministic=False):
+    """`config` of the JSON line (the same for both arms)."""
+    M = w["spokes"] * w["samples"]
+    return {"workload": workload_name(w), "samples_per_step_per_gpu": 2 * w["coils"] * M,
+            "grid": [math.ceil(w["oversamp"] * w["N"])] * 3,
+            "gridding": "deterministic" if deterministic else "atomic",
+            "l2": "inputs larger than L2 (image 1.8 GB, k-space 4.9 GB per GPU)"
+            if not (args.small or args.medium) else "inputs larger than L2",
+            "parallelism": f"replicas x{world} (one independent workload per GPU)"}
+
+
 def alg_bytes(w, M):
     """Compulsory bytes of one interpolation / gridding launch (complex64 samples and
     grid, float32 coordinates, float32 density weight for gridding)."""
@@ -356,15 +393,18 @@ def run_b200(args):
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "alg_bytes_per_launch": kbytes}
 
-    # serving after the end-to-end leg: its request sets and slots stay out of the e2e timing
-    serving = None
+    # serving and the other configurations after the end-to-end leg: their
+    # buffers stay out of the e2e timing
+    serving = others = None
     if not args.no_extras and rank == 0:
         serving = run_serving(dev)
+        others = run_other_configs(dev, max(3, args.steps // 2))
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = CpuBaseline(w)
         cpu = cb.info(cb.run())
+        parity = parity_check(F, cb, plan, img, ksp, dcf)
 
     if rank == 0:
         line = {
@@ -372,20 +412,151 @@ def run_b200(args):
             "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (complex64)",
             "data": "synthetic, seeded (golden-means kooshball, complex Gaussian image and k-space, ramp density weights)",
-            "config": {"workload": workload_name(w), "samples_per_step_per_gpu": samples_step,
-                       "grid": [math.ceil(w["oversamp"] * N)] * 3,
-                       "gridding": "deterministic" if F.deterministic_gridding() else "atomic",
-                       "l2": "inputs larger than L2 (image 1.8 GB, k-space 4.9 GB per GPU)"
-                       if not args.small else "inputs larger than L2",
-                       "parallelism": f"replicas x{world} (one independent workload per GPU)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": ck, "extras": extras, "serving": serving,
+            "config": bench_config(w, args, world, F.deterministic_gridding()),
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": ck, "extras": extras, "serving": serving, "other_configs": others,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# the other configurations: 2D radial, batched uneven frames, differentiable DC
+# ---------------------------------------------------------------------------
+def _timed_events(fn, n, warm=3):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(n):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / n
+
+
+def nudft2d_fp64(img, coord, n):
+    """Direct NUDFT y[b, p] = sum_x img[b, x] exp(-2 pi i k.(x - N//2) / N) in
+    float64 on the GPU (coord in grid units, (x, y); image axes (y, x)),
+    separable over the two axes, in chunks of samples."""
+    dev = img.device
+    x = img.to(torch.complex128)
+    idx = torch.arange(n, device=dev, dtype=torch.float64) - n // 2
+    c = torch.as_tensor(coord, device=dev, dtype=torch.float64).reshape(-1, 2)
+    out = []
+    for s in range(0, c.shape[0], 8192):
+        cc = c[s:s + 8192]
+        ex = torch.exp(-2j * math.pi * cc[:, 0:1] * idx[None, :] / n)  # (m, nx)
+        ey = torch.exp(-2j * math.pi * cc[:, 1:2] * idx[None, :] / n)  # (m, ny)
+        t = torch.einsum("byx,mx->bym", x, ex)
+        out.append(torch.einsum("bym,my->bm", t, ey))
+    return torch.cat(out, dim=1)
+
+
+def run_other_configs(dev, steps):
+    """Throughput of the other workload configurations with inputs resident in
+    HBM (CUDA events, current stream), next to their plain or per-call forms."""
+    import deepmr_b200.fft as F
+    from deepmr_b200 import synth
+
+    peak, _ = measured_peak()
+    out = {}
+
+    # 2D golden-angle radial: 128^2, 8 coils, 256 x 256 samples, width 3, oversampling 2
+    N, C = 128, 8
+    c = synth.radial_2d(256, 256, N)
+    dcf = torch.as_tensor(synth.ramp_dcf(c)).to(dev)
+    plan = F.plan_nufft(torch.as_tensor(c), N, 3, 2.0, device=dev)
+    img = synth.complex_gaussian((C, N, N), seed=31, device=dev)
+    ksp = synth.complex_gaussian((C,) + tuple(c.shape[:-1]), seed=32, device=dev)
+    M = c.shape[0] * c.shape[1]
+    eager = _timed_events(lambda: (F.apply_nufft(img, plan), F.apply_nufft_adj(ksp, plan, weight=dcf)), 10 * steps)
+    op = F.CapturedNUFFT(plan, batch=C, weight=dcf.reshape(-1))
+    graph = _timed_events(lambda: (op.forward(img), op.adjoint(ksp)), 10 * steps)
+    y = F.apply_nufft(img, plan)
+    ref = nudft2d_fp64(img, c, N)
+    yv = y.reshape(C, -1).to(torch.complex128)
+    raw = float(torch.linalg.norm(yv - ref) / torch.linalg.norm(ref))
+    scale = torch.vdot(yv.flatten(), ref.flatten()) / torch.vdot(yv.flatten(), yv.flatten())
+    fitted = float(torch.linalg.norm(scale * yv - ref) / torch.linalg.norm(ref))
+    out["radial2d_128_8coils"] = {
+        "workload": "2D golden-angle radial 128^2, 8 coils, 256 spokes x 256 samples, KB width 3, "
+                    "oversampling 2, ramp density weights: forward + adjoint",
+        "samples_per_s": 2 * C * M / (eager / 1e3), "ms_per_pair": eager,
+        "captured_graph": {"samples_per_s": 2 * C * M / (graph / 1e3), "ms_per_pair": graph},
+        "nudft_fp64": {"rel_l2": raw, "rel_l2_after_global_scale_fit": fitted, "global_scale": abs(complex(scale)),
+                       "note": "forward of all 8 coils at all 65,536 samples against a float64 direct NUDFT "
+                               "on the GPU (the kernel's own approximation error at width 3, oversampling 2)"}}
+    del plan, img, ksp, op, y, ref, yv
+    torch.cuda.empty_cache()
+
+    # batched uneven frames: 224^2, 16 coils, 500 spiral frames of U{800..1200} samples
+    N, C, NF = 224, 16, 500
+    rng = np.random.default_rng(3)
+    coords = [synth.spiral_2d(int(L), N, rotation=f * synth.GOLDEN_ANGLE)[0]
+              for f, L in enumerate(rng.integers(800, 1201, NF))]
+    total = sum(x.shape[0] for x in coords)
+    plan = F.plan_nufft(coords, N, 4, 1.25, device=dev)
+    img = synth.complex_gaussian((C, NF, N, N), seed=41, device=dev)
+    ksp = synth.complex_gaussian((C, total), seed=42, device=dev)
+    batched = _timed_events(lambda: (F.apply_nufft(img, plan), F.apply_nufft_adj(ksp, plan)), steps)
+    op = F.CapturedNUFFT(plan, batch=C)
+    graph = _timed_events(lambda: (op.forward(img), op.adjoint(ksp)), steps)
+    del op
+    torch.cuda.empty_cache()
+    plans = [F.plan_nufft(torch.as_tensor(x), N, 4, 1.25, device=dev) for x in coords]
+    offs = np.concatenate([[0], np.cumsum([x.shape[0] for x in coords])])
+    kparts = [ksp[:, offs[f]:offs[f + 1]].reshape(C, 1, -1) for f in range(NF)]
+
+    def per_frame():
+        for f in range(NF):
+            F.apply_nufft(img[:, f], plans[f])
+            F.apply_nufft_adj(kparts[f], plans[f])
+
+    plain = _timed_events(per_frame, max(1, steps // 2), warm=1)
+    alg = 2 * (8 * C * NF * N * N + 4 * 2 * total + 8 * C * total)
+    out["uneven_frames_224_16coils_500frames"] = {
+        "workload": f"500 variable-density spiral frames of U{{800..1200}} samples ({total} in all), 224^2, "
+                    "16 coils, KB width 4, oversampling 1.25: forward + adjoint of all frames",
+        "batched": {"samples_per_s": 2 * C * total / (batched / 1e3), "ms_per_pair": batched,
+                    "hbm_frac_of_measured": alg / (batched / 1e3) / 1e9 / peak},
+        "batched_captured_graph": {"samples_per_s": 2 * C * total / (graph / 1e3), "ms_per_pair": graph},
+        "per_frame_calls": {"samples_per_s": 2 * C * total / (plain / 1e3), "ms_per_pair": plain,
+                            "note": "500 plans, one apply_nufft + apply_nufft_adj call per frame"},
+        "alg_bytes_per_pair": alg}
+    del plan, plans, img, ksp, kparts
+    torch.cuda.empty_cache()
+
+    # differentiable data consistency: 256^2, 12 coils, 402 x 512 radial, gradients of
+    # ||A x - y||^2 with respect to the image and the trajectory
+    N, C = 256, 12
+    c = synth.radial_2d(402, 512, N)
+    coord = torch.as_tensor(c).to(dev)
+    x = synth.complex_gaussian((C, N, N), seed=51, device=dev)
+    yobs = synth.complex_gaussian((C,) + tuple(c.shape[:-1]), seed=52, device=dev)
+    M = c.shape[0] * c.shape[1]
+
+    def dc_step():
+        xx = x.clone().requires_grad_(True)
+        cc = coord.clone().requires_grad_(True)
+        r = F.nufft(xx, cc, width=4, oversamp=1.25, device=dev) - yobs
+        loss = (r.real**2 + r.imag**2).sum()
+        loss.backward()
+        return xx.grad, cc.grad
+
+    dc = _timed_events(dc_step, steps)
+    out["dc_gradients_256_12coils"] = {
+        "workload": "2D radial 256^2, 12 coils, 402 spokes x 512 samples, KB width 4, oversampling 1.25: "
+                    "loss ||A x - y||^2 and its gradients w.r.t. the image and the trajectory (plan, forward, "
+                    "adjoint, trajectory-gradient kernel)",
+        "ms_per_step": dc, "samples_per_s": C * M / (dc / 1e3)}
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -425,13 +596,20 @@ def run_serving(dev, nreq=64, seed=0, max_active=4):
 # reference arm: CPU restatement of the reference, host cores
 # ---------------------------------------------------------------------------
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle port: C loops with OpenMP over
+    (frame, coil) for gridding and over samples for interpolation, torch CPU
+    FFTs) on the host cores. Each step is one forward + adjoint pair over the
+    full trajectory for as many coils as there are host threads (at most the
+    workload's 32), so the per-(frame, coil) gridding keeps every core busy;
+    time is linear in the coil count, and `value` is samples per second like
+    the GPU arm's."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = workload(args)
     cores = os.cpu_count() or 1
-    cb = CpuBaseline(w, max(1, min(cores, 8, w["coils"])))
+    cb = CpuBaseline(w, max(1, min(cores, w["coils"])))
     coils = cb.coils
     for _ in range(max(args.warmup, 0)):
         cb.run()
@@ -440,12 +618,14 @@ def run_reference(args):
     samples = coils * w["spokes"] * w["samples"] * 2
     value = samples * len(times) / sum(times)
     info["value"] = value
+    info["sample"] = (f"{coils} of {w['coils']} coils per step (one per host thread), full trajectory; "
+                      + info["sample"])
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (complex64)",
-        "data": "synthetic, seeded", "config": {"workload": workload_name(w),
-                                                 "sample": f"{coils} of {w['coils']} coils per step"},
+        "data": "synthetic, seeded (golden-means kooshball, complex Gaussian image and k-space, ramp density weights)",
+        "config": bench_config(w, args, world),
         "cpu_baseline": info, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                                       "d2h_bytes_per_step": 0},
     }

@@ -23,6 +23,7 @@ ERRORS = {
     -5: "DMR_ERR_CUFFT",
     -6: "DMR_ERR_UNSUPPORTED",
     -7: "DMR_ERR_WORKSPACE",
+    -8: "DMR_ERR_TIMEOUT",
 }
 
 # every symbol declared in include/deepmr_b200.h
@@ -31,6 +32,8 @@ SYMBOLS = (
     "dmr_last_error",
     "dmr_launch_count",
     "dmr_tc_timeouts",
+    "dmr_plan_status",
+    "dmr_tc_test_stall",
     "dmr_detect_cartesian",
     "dmr_plan_create",
     "dmr_plan_destroy",
@@ -81,6 +84,8 @@ _SIGS = {
     "dmr_last_error": (ctypes.c_char_p, []),
     "dmr_launch_count": (i64, []),
     "dmr_tc_timeouts": (ctypes.c_int, [i64p, ctypes.c_int]),
+    "dmr_plan_status": (ctypes.c_int, [vp, i32p, ctypes.c_int, vp]),
+    "dmr_tc_test_stall": (ctypes.c_int, [ctypes.c_int]),
     "dmr_detect_cartesian": (ctypes.c_int, [vp, i64, ctypes.c_int, i32p, i32p, vp]),
     "dmr_plan_create": (
         ctypes.c_int,

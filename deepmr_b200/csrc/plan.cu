@@ -116,6 +116,14 @@ __global__ void gather_sorted_kernel(int64_t total, int ndim, const int32_t *__r
     }
 }
 
+// sort key (frame, bin, cell) -> (frame, bin)
+__global__ void bin_key_kernel(int64_t total, int cells, int32_t *__restrict__ keys)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        keys[i] /= cells;
+}
+
 static int grid_blocks(int64_t n, int threads)
 {
     int dev = 0, sms = 148;
@@ -352,6 +360,8 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
         DMR_TRY(dev_alloc(&p->scoord[a], total));
     }
     DMR_TRY(dev_alloc(&p->sidx, total));
+    DMR_TRY(dev_alloc(&p->status, 1));
+    DMR_CUDA(cudaMemsetAsync(p->status, 0, sizeof(int32_t), st));
     DMR_CUDA(cudaMemsetAsync(counts, 0, nkeys * sizeof(int32_t), st));
     DMR_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
     DMR_CUDA(cudaMemcpyAsync(d_foff, frame_offsets, (nframes + 1) * sizeof(int64_t),
@@ -382,6 +392,32 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
         gather_sorted_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
             total, ndim, p->sidx, rk[0], rk[1], rk[2], p->scoord[0], p->scoord[1], p->scoord[2]);
         DMR_LAUNCHED("gather_sorted_kernel");
+        // 3D: the same bins in acquisition order (stable sort by (frame, bin) alone)
+        if (ndim == 3 && cell_order) {
+            const int cells = g.T[0] * g.T[1] * g.T[2];
+            bin_key_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(total, cells, keys);
+            DMR_LAUNCHED("bin_key_kernel");
+            int bin_bit = 1;
+            while ((1ll << bin_bit) < nkeys) bin_bit++;
+            for (int a = 0; a < 3; a++) DMR_TRY(dev_alloc(&p->acq_scoord[a], total));
+            DMR_TRY(dev_alloc(&p->acq_sidx, total));
+            p->acq_owned = true;
+            size_t tb2 = 0;
+            DMR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, keys, keys_s, vals, p->acq_sidx,
+                                                     (int)total, 0, bin_bit, st));
+            DMR_CHECK(tb2 <= std::max<size_t>(temp_bytes, 1), DMR_ERR_INVALID, "sort scratch");
+            DMR_CUDA(cub::DeviceRadixSort::SortPairs(temp, tb2, keys, keys_s, vals, p->acq_sidx,
+                                                     (int)total, 0, bin_bit, st));
+            g_launches.fetch_add(1);
+            gather_sorted_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
+                total, ndim, p->acq_sidx, rk[0], rk[1], rk[2], p->acq_scoord[0], p->acq_scoord[1],
+                p->acq_scoord[2]);
+            DMR_LAUNCHED("gather_sorted_kernel");
+        }
+    }
+    if (!p->acq_owned) {
+        for (int a = 0; a < 3; a++) p->acq_scoord[a] = p->scoord[a];
+        p->acq_sidx = p->sidx;
     }
 
     std::vector<int32_t> h_counts(nkeys);

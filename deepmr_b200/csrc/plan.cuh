@@ -73,6 +73,10 @@ size_t rt_scratch_bytes(const ::dmr_plan *p, int64_t batch);
 // the bin region does not fit
 int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, cudaStream_t st);
+// the same with the spreading operand in tensor memory (tmgrid.cu); `timeouts`
+// is the device address of the process-wide counter of blocks that stopped
+int grid_tm_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
+                     const float *weight, int wpb, int *timeouts, int stall, cudaStream_t st);
 
 }  // namespace dmr
 
@@ -85,6 +89,12 @@ struct dmr_plan {
     // device buffers
     float *scoord[3] = {nullptr, nullptr, nullptr};  // sorted rescaled coordinates
     int32_t *sidx = nullptr;            // sorted position -> global sample index
+    // 3D plans: the same bins with their samples in acquisition order (the
+    // tensor-core gridding reads consecutive samples of a spoke together);
+    // alias scoord / sidx when the plan's own order already is that
+    float *acq_scoord[3] = {nullptr, nullptr, nullptr};
+    int32_t *acq_sidx = nullptr;
+    bool acq_owned = false;
     int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
     dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
     int nwork = 0;
@@ -104,6 +114,9 @@ struct dmr_plan {
     dmr::RtItem *rt_reduce = nullptr;
     int nrt_reduce = 0;
     int rt_slots = 0;
+    // device status word: blocks of this plan's calls whose bounded wait ran out
+    // (dmr_plan_status; 0 while every result is valid)
+    int32_t *status = nullptr;
 
     ~dmr_plan()
     {
@@ -112,6 +125,10 @@ struct dmr_plan {
             cudaFree(apod[a]);
         }
         cudaFree(sidx);
+        if (acq_owned) {
+            for (int a = 0; a < 3; a++) cudaFree(acq_scoord[a]);
+            cudaFree(acq_sidx);
+        }
         cudaFree(bin_start);
         cudaFree(work);
         cudaFree(work_order);
@@ -120,5 +137,6 @@ struct dmr_plan {
         cudaFree(foff_dev);
         cudaFree(rt_items);
         cudaFree(rt_reduce);
+        cudaFree(status);
     }
 };

@@ -33,14 +33,19 @@
 // Pipeline: A and B are double-buffered; the MMAs of one chunk run while the
 // threads build the next, and a buffer is rebuilt only after the mbarrier
 // signalled by tcgen05.commit for the chunk that last read it. Every wait is
-// bounded: a wait that runs out sets a device flag, and the block stops
-// issuing work and frees its tensor memory.
+// bounded in time (%globaltimer): a wait that runs out makes the block stop
+// issuing work, wait (again bounded) for its own MMAs in flight, free its
+// tensor memory and count itself in the plan's status word, which the host
+// reads with dmr_plan_status (the call's result is then not valid).
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 #include <cstdint>
 #include <cstdlib>
 
 #include "kb.cuh"
 #include "plan.cuh"
+#include "tcgen05.cuh"
 
 namespace dmr {
 
@@ -53,71 +58,13 @@ constexpr int kTcMaxMT = 4;           // 128-point tiles (P <= 512)
 constexpr int kTcMaxCC = 32;          // coils per block (N <= 64)
 static_assert(kTcMaxCC * kTcSC <= kTcThreads, "one (coil, sample) of a chunk per thread");
 constexpr int kTcPairs = (2 * kTcMaxMT * 128 + kTcThreads - 1) / kTcThreads;  // A-build pairs per thread
-constexpr int kTcRowBytes = kTcK * 32;        // 512: stride between 8-row core-matrix groups
+static_assert(kTcRowBytes == kTcK * 32, "stride between 8-row core-matrix groups");
 constexpr int kTcTileBytes = 16 * kTcRowBytes;  // 8192: one 128-row operand tile
-constexpr long long kTcSpin = 1ll << 20;      // bound on mbarrier polls
+constexpr uint64_t kTcWaitNs = 200000000ull;   // bound on an operand-buffer wait (200 ms)
+constexpr uint64_t kTcDrainNs = 2000000000ull; // bound on the wait before tensor memory is freed (2 s)
+constexpr uint64_t kTcStallNs = 1000000ull;    // test stall: wait on a barrier nothing signals (1 ms)
 
-__device__ int g_tc_timeouts = 0;  // waits that ran out (should stay 0)
-
-__device__ __forceinline__ uint32_t tc_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ uint64_t tc_desc(uint32_t addr)
-{
-    // start address, leading byte offset 128, stride byte offset 512, version 1, no swizzle
-    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
-           ((uint64_t)(kTcRowBytes >> 4) << 32) | (1ull << 46);
-}
-
-// hi part of the split: x with the 13 mantissa bits that tf32 drops cleared
-// (exactly representable, so lo = x - hi is exact and |lo| < 2^-10 |x|)
-__device__ __forceinline__ float tc_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
-
-__device__ __forceinline__ float4 tc_lds4(uint32_t a)
-{
-    float4 v;
-    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
-    return v;
-}
-
-__device__ __forceinline__ void tc_sts4(uint32_t a, float4 v)
-{
-    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_sts(uint32_t a, float v)
-{
-    asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
-}
-
-__device__ __forceinline__ bool tc_try_wait(uint32_t bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// bounded wait for completion number k (parity k & 1) of an mbarrier
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t k)
-{
-    for (long long i = 0; i < kTcSpin; i++)
-        if (tc_try_wait(bar, k & 1)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16])
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-}
+__device__ int g_tc_timeouts = 0;  // blocks whose wait ran out, all plans (should stay 0)
 
 struct TcShape {
     int R[3];    // region extents (T + W - 1)
@@ -139,10 +86,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
     Geom g, TcShape sh, const WorkItem *__restrict__ work, const int32_t *__restrict__ order, int nwork, int nchunks,
     const float *__restrict__ sc0, const float *__restrict__ sc1, const float *__restrict__ sc2,
     const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid,
-    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale)
+    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale, int *__restrict__ status,
+    int stall)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    // mbar[0..1]: operand buffers; mbar[2]: never signalled (test stall)
+    __shared__ __align__(8) uint64_t mbar[3];
     __shared__ uint32_t tslot;
     __shared__ int s_abort;
 
@@ -168,6 +117,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mbar[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mbar[1])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mbar[2])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_abort = 0;
     }
@@ -296,7 +246,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
                 const uint32_t nuse = buf ? uses1 : uses0;
                 if (chunk_no >= 2) {
                     // the MMAs of chunk chunk_no - 2 read this buffer
-                    if (!tc_wait(bar, nuse - 1)) s_abort = 1;
+                    if (!tc_wait(bar, nuse - 1, kTcWaitNs)) s_abort = 1;
+                    // test hook: a barrier that no commit signals, so this wait runs out
+                    if (stall && !tc_wait(tc_smem(&mbar[2]), 0, kTcStallNs)) s_abort = 1;
                 }
                 const int s0 = ch * kTcSC;
                 // A: thread per (point, sample quad), addresses precomputed
@@ -365,7 +317,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
         // epilogue: wait for the last chunk, read the accumulators, add to the grid
         {
             const int lb = (chunk_no - 1) & 1;
-            if (!tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1)) s_abort = 1;
+            if (!tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1, kTcWaitNs)) s_abort = 1;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         __syncthreads();
@@ -408,11 +360,19 @@ __global__ void __launch_bounds__(kTcThreads, 2) grid_tc_kernel(
         // the next task's first MMAs overwrite the accumulator after its build barrier
     }
 done:
-    if (s_abort && tid == 0) atomicAdd(&g_tc_timeouts, 1);
-    // let the last commit land before the tensor memory is released (bounded)
-    if (tid == 0 && chunk_no > 0) {
-        const int lb = (chunk_no - 1) & 1;
-        tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1);
+    // let the last commit land before the tensor memory is released (bounded;
+    // if even this wait runs out the block is counted as failed, since its
+    // MMAs may still write the columns it frees)
+    if (tid == 0) {
+        bool fail = s_abort != 0;
+        if (chunk_no > 0) {
+            const int lb = (chunk_no - 1) & 1;
+            if (!tc_wait(bar0 + 8 * lb, (lb ? uses1 : uses0) - 1, kTcDrainNs)) fail = true;
+        }
+        if (fail) {
+            atomicAdd(&g_tc_timeouts, 1);
+            atomicAdd(status, 1);
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -427,6 +387,29 @@ static int tc_disabled()
         return e && atoi(e) ? 1 : 0;
     }();
     return v;
+}
+
+static std::atomic<int> g_tc_stall{0};  // test hook (dmr_tc_test_stall)
+
+static int tm_disabled()
+{
+    static const int v = [] {
+        const char *e = getenv("DMR_NO_TMEM_A");
+        return e && atoi(e) ? 1 : 0;
+    }();
+    return v;
+}
+
+// device address of g_tc_timeouts, looked up once per device (that device current)
+static int timeouts_ptr(int dev, int **out)
+{
+    static std::mutex mu;
+    static int *ptrs[64] = {};
+    DMR_CHECK(dev >= 0 && dev < 64, DMR_ERR_UNSUPPORTED, "device index %d", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) DMR_CUDA(cudaGetSymbolAddress((void **)&ptrs[dev], g_tc_timeouts));
+    *out = ptrs[dev];
+    return DMR_OK;
 }
 
 static bool tc_shape(const Geom &g, int64_t batch, TcShape &s)
@@ -451,34 +434,63 @@ static bool tc_shape(const Geom &g, int64_t batch, TcShape &s)
 int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, cudaStream_t st)
 {
-    TcShape sh;
-    if (tc_disabled() || !tc_shape(p->g, batch, sh)) return DMR_ERR_UNSUPPORTED;
-    int dev = 0, sms = 0, smem_sm = 0, smem_blk = 0;
+    if (tc_disabled()) return DMR_ERR_UNSUPPORTED;
+    int dev = 0;
     DMR_CUDA(cudaGetDevice(&dev));
+    if (!tm_disabled()) {
+        int *timeouts = nullptr;
+        DMR_TRY(timeouts_ptr(dev, &timeouts));
+        const int rc = grid_tm_dispatch(p, ksp, kreal, grid, batch, weight, wpb, timeouts, g_tc_stall.load(), st);
+        if (rc != DMR_ERR_UNSUPPORTED) return rc;
+    }
+    TcShape sh;
+    if (!tc_shape(p->g, batch, sh)) return DMR_ERR_UNSUPPORTED;
+    int sms = 0, smem_sm = 0, smem_blk = 0, reserved = 0;
     DMR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     DMR_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     DMR_CUDA(cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    DMR_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
     size_t smem = tc_smem_bytes(sh);
+    DMR_CHECK(smem <= (size_t)smem_blk, DMR_ERR_UNSUPPORTED, "tensor-core gridding needs %zu B of shared memory", smem);
+    {
+        // the dynamic maximum leaves room for the kernel's static shared memory
+        cudaFuncAttributes fa;
+        DMR_CUDA(cudaFuncGetAttributes(&fa, grid_tc_kernel));
+        smem_blk -= (int)fa.sharedSizeBytes;
+        if (smem > (size_t)smem_blk) return DMR_ERR_UNSUPPORTED;
+        DMR_CUDA(cudaFuncSetAttribute(grid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_blk));
+    }
+    // (set back to the size launched below: a larger maximum can make the
+    // driver reserve more shared memory and leave less L1 cache)
     // resident blocks of one SM must not ask for more than its 512 tensor-memory
-    // columns: pad the shared memory so that at most 512 / ncols blocks fit
+    // columns (a block that found none free would wait in tcgen05.alloc until a
+    // co-resident block exits): pad the dynamic shared memory until the
+    // occupancy calculator admits at most 512 / ncols blocks per SM
     const int maxb = 512 / sh.ncols;
-    const size_t reserve = 2048 + 64;  // per-block driver reserve + static shared memory
-    // (padded with 1 KB to spare, so maxb + 1 blocks cannot fit whatever the
-    // allocation granularity; a block that found no free columns would wait in
-    // tcgen05.alloc until a co-resident block exits)
-    if ((size_t)smem_sm / (smem + reserve) > (size_t)maxb) smem = (size_t)smem_sm / (maxb + 1) - 1024;
-    if (smem > (size_t)smem_blk) return DMR_ERR_UNSUPPORTED;
-    const int per_sm = std::max(1, std::min(maxb, (int)((size_t)smem_sm / (smem + reserve))));
+    int per_sm = 0;
+    DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tc_kernel, kTcThreads, smem));
+    if (per_sm > maxb) {
+        const size_t fit = (size_t)smem_sm / (maxb + 1);  // per-block share if maxb + 1 blocks fit
+        smem = std::max(smem, fit > (size_t)reserved ? fit - (size_t)reserved : smem);
+        DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tc_kernel, kTcThreads, smem));
+        while (per_sm > maxb && smem + 1024 <= (size_t)smem_blk) {
+            smem += 1024;
+            DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tc_kernel, kTcThreads, smem));
+        }
+        if (per_sm > maxb) return DMR_ERR_UNSUPPORTED;
+    }
+    DMR_CHECK(per_sm >= 1, DMR_ERR_UNSUPPORTED, "tensor-core gridding: no resident block");
+    DMR_CUDA(cudaFuncSetAttribute(grid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->nwork == 0) return DMR_OK;
     const int64_t nchunks = ceil_div(batch, sh.CC);
     const int64_t tasks = (int64_t)p->nwork * nchunks;
     DMR_CHECK(tasks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
     const int blocks = (int)std::min<int64_t>(tasks, (int64_t)sms * per_sm);
-    DMR_CUDA(cudaFuncSetAttribute(grid_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     grid_tc_kernel<<<blocks, kTcThreads, smem, st>>>(p->g, sh, p->work, p->work_order, p->nwork, (int)nchunks, p->scoord[0],
                                                       p->scoord[1], p->scoord[2], p->sidx, ksp, kreal, grid,
-                                                      batch, weight, wpb, (float)(1.0 / p->scale));
+                                                      batch, weight, wpb, (float)(1.0 / p->scale), p->status,
+                                                      g_tc_stall.load());
     DMR_LAUNCHED("grid_tc_kernel");
     return DMR_OK;
 }
@@ -498,5 +510,29 @@ extern "C" int dmr_tc_timeouts(int64_t *count, int reset)
         const int zero = 0;
         DMR_CUDA(cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)));
     }
+    return DMR_OK;
+}
+
+extern "C" int dmr_tc_test_stall(int enable)
+{
+    g_tc_stall.store(enable ? 1 : 0);
+    return DMR_OK;
+}
+
+extern "C" int dmr_plan_status(dmr_plan *p, int32_t *failed, int reset, void *stream)
+{
+    DMR_CHECK(p, DMR_ERR_INVALID, "NULL plan");
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t v = 0;
+    DMR_CUDA(cudaMemcpyAsync(&v, p->status, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    DMR_CUDA(cudaStreamSynchronize(st));
+    if (failed) *failed = v;
+    if (reset && v) {
+        DMR_CUDA(cudaMemsetAsync(p->status, 0, sizeof(int32_t), st));
+        DMR_CUDA(cudaStreamSynchronize(st));
+    }
+    DMR_CHECK(v == 0, DMR_ERR_TIMEOUT,
+              "%d tensor-core gridding block(s) of this plan stopped on a bounded wait that ran out: "
+              "the results of the calls since the last reset are not valid", (int)v);
     return DMR_OK;
 }

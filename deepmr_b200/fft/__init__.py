@@ -45,6 +45,7 @@ __all__ = [
     "GramMatrix",
     "set_deterministic_gridding",
     "deterministic_gridding",
+    "set_status_check",
     "traj_grad",
     "CapturedNUFFT",
     "frames_split",
@@ -76,6 +77,14 @@ def set_deterministic_gridding(flag=True):
 def deterministic_gridding():
     """Current gridding mode (see set_deterministic_gridding)."""
     return _nufft.DETERMINISTIC_GRIDDING
+
+
+def set_status_check(flag=True):
+    """Also check the gridding's device status (a bounded wait that ran out
+    raises DmrError DMR_ERR_TIMEOUT) after adjoint calls whose result stays on
+    the GPU, at one stream synchronisation per call. Calls whose result returns
+    to the host are always checked. Returns the previous setting."""
+    return _nufft.set_status_check(flag)
 
 
 def nufft(image, coord, shape=None, basis_adjoint=None, device="cpu", threadsperblock=128,

@@ -122,6 +122,16 @@ class DevicePlan:
             self._build()
         return self
 
+    def check_status(self, reset=True):
+        """Raise ``DmrError`` (DMR_ERR_TIMEOUT) if a tensor-core gridding block of
+        this plan's calls stopped on a bounded device wait since the last reset
+        (the results of those calls are then partial). Synchronises the current
+        stream of the plan's device; ``reset`` clears the status."""
+        n = ctypes.c_int32()
+        with torch.cuda.device(self.device):
+            _lib.check(_lib.lib().dmr_plan_status(self.handle, ctypes.byref(n), int(bool(reset)),
+                                                  _lib.stream_ptr(self.device)))
+
     def workspace(self, batch):
         n = ctypes.c_size_t()
         with torch.cuda.device(self.device):
@@ -378,6 +388,19 @@ def _as_cfloat(x):
 # with global atomics; True = fixed-order owner tiles (bitwise reproducible).
 DETERMINISTIC_GRIDDING = False
 
+# Device status of the gridding (a bounded wait that ran out, DMR_ERR_TIMEOUT)
+# is checked after every adjoint whose result returns to the host (that call
+# synchronises anyway); True also checks after device-resident calls (one
+# stream synchronisation each). DevicePlan.check_status checks on demand.
+CHECK_STATUS = False
+
+
+def set_status_check(on):
+    """Check the gridding status after every adjoint call; returns the old setting."""
+    global CHECK_STATUS
+    old, CHECK_STATUS = CHECK_STATUS, bool(on)
+    return old
+
 
 def _basis_arg(basis, rows, cols, dev, name):
     """Subspace matrix as a contiguous complex64 device tensor of shape (rows, cols)
@@ -598,6 +621,7 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
         out = torch.empty([batch] + item, dtype=torch.complex64, pin_memory=True)
         _pipelined(kspace.reshape((batch,) + tuple(kspace.shape[len(batch_shape):])), out, batch, dev, run,
                    interp.workspace, min_chunk)
+        interp.check_status()
         return out.reshape(list(batch_shape) + item)
     y = kspace.to(dev).contiguous()
     out = torch.empty(list(batch_shape) + item, dtype=torch.complex64, device=dev)
@@ -606,6 +630,8 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
         with torch.cuda.device(dev):
             run(y, out, 0, batch, interp.workspace(batch), _lib.stream_ptr(dev))
     out = _to_origin(out, kspace)
+    if batch > 0 and (CHECK_STATUS or out.device.type == "cpu"):
+        interp.check_status()
     return out.numpy(force=True) if isnumpy else out
 
 
@@ -678,6 +704,8 @@ def _apply_nufft_adj_lowrank(kspace, nufft_plan, basis, weight, device, determin
                 interp.handle, _lib.ptr(y), int(not y.is_complex()), ncoeff, _lib.ptr(bb), _lib.ptr(out), batch,
                 _lib.ptr(w), wpb, det, _lib.ptr(ws), ws.numel(), _lib.stream_ptr(dev)))
     out = _to_origin(out, kspace)
+    if batch > 0 and (CHECK_STATUS or out.device.type == "cpu"):
+        interp.check_status()
     return out.numpy(force=True) if isnumpy else out
 
 

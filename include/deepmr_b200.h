@@ -44,6 +44,7 @@ extern "C" {
 #define DMR_ERR_CUFFT -5       /* cuFFT error */
 #define DMR_ERR_UNSUPPORTED -6 /* configuration not supported */
 #define DMR_ERR_WORKSPACE -7   /* workspace too small */
+#define DMR_ERR_TIMEOUT -8     /* a bounded device-side wait ran out: results not valid */
 
 typedef struct dmr_plan dmr_plan;
 
@@ -57,12 +58,33 @@ const char *dmr_last_error(void);
 int64_t dmr_launch_count(void);
 
 /*
- * Bounded waits of the tensor-core gridding kernel that ran out on the current
- * device since load (each such block stops issuing work and frees its tensor
+ * Blocks of the tensor-core gridding kernel, over all plans on the current
+ * device since load, that stopped because a bounded wait ran out (each such
+ * block stops issuing work, waits for its MMAs in flight and frees its tensor
  * memory; the count should stay 0). Reads after a device synchronisation;
  * reset != 0 zeroes the counter. No reference counterpart (device health).
  */
 int dmr_tc_timeouts(int64_t *count, int reset);
+
+/*
+ * Device status of a plan: `failed` (host, may be NULL) receives the number of
+ * gridding blocks of this plan's calls that stopped on a bounded wait since
+ * the last reset. Synchronises `stream`; returns DMR_ERR_TIMEOUT when that
+ * number is non-zero (the outputs of the calls since the last reset are then
+ * partial and must not be used), DMR_OK otherwise; reset != 0 zeroes it.
+ * Calls on one plan from several streams share the word. No reference
+ * counterpart (the reference's kernels have no device-side waits).
+ */
+int dmr_plan_status(dmr_plan *plan, int32_t *failed, int reset, void *stream);
+
+/*
+ * Test hook, no reference counterpart: enable != 0 makes every block of the
+ * following tensor-core gridding launches (all plans) wait, before it reuses
+ * an operand buffer, on an mbarrier that nothing signals, so that the bounded
+ * wait (1 ms) runs out and the block stops; enable = 0 restores normal runs.
+ * Exercises the timeout path without a GPU fault.
+ */
+int dmr_tc_test_stall(int enable);
 
 /*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):

@@ -19,13 +19,16 @@ def golden_cases(prefix=None, kind="nufft"):
     toep = [n for n in names if n.startswith("toep")]
     lowrank = [n for n in names if n.startswith("lowrank")]
     sparse = [n for n in names if n.startswith("sparse")]
+    cgsense = [n for n in names if n.startswith("cgsense")]
+    if kind == "cgsense":
+        return cgsense
     if kind == "toeplitz":
         return toep
     if kind == "lowrank":
         return lowrank
     if kind == "sparse":
         return sparse
-    return [n for n in names if n not in toep and n not in lowrank and n not in sparse]
+    return [n for n in names if n not in toep and n not in lowrank and n not in sparse and n not in cgsense]
 
 
 @pytest.fixture

@@ -1,9 +1,10 @@
 """Generate golden NUFFT vectors by running the reference implementation.
 
-Run in a container where the reference project is available (read-only) at
-``/root/reference``::
+Run where the reference project is available (read-only); its location is
+the ``DEEPMR_REFERENCE`` environment variable (the project root, containing
+``src/deepmr``), or ``--reference PATH``::
 
-    python tests/golden/make_golden.py            # every case
+    DEEPMR_REFERENCE=/path/to/deep-mr python tests/golden/make_golden.py   # every case
     python tests/golden/make_golden.py lowrank    # only the low-rank cases
     python tests/golden/make_golden.py sparse     # only the sparse FFT cases
 
@@ -29,7 +30,19 @@ import types
 os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="numba_"))
 sys.dont_write_bytecode = True
 
-REF_SRC = "/root/reference/src/deepmr"
+def _reference_root():
+    if "--reference" in sys.argv:
+        i = sys.argv.index("--reference")
+        root = sys.argv[i + 1]
+        del sys.argv[i:i + 2]
+        return root
+    root = os.environ.get("DEEPMR_REFERENCE")
+    if not root:
+        raise SystemExit("set DEEPMR_REFERENCE (or pass --reference) to the reference project's root")
+    return root
+
+
+REF_SRC = os.path.join(_reference_root(), "src", "deepmr")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 
@@ -50,6 +63,61 @@ def import_reference():
     import deepmr.fft  # noqa: F401
 
     return sys.modules["deepmr.fft.nufft"], sys.modules["deepmr.fft"]
+
+
+def import_reference_recon():
+    """The reference's linear operators, CG and encoding-operator builder
+    (deepmr.linops, deepmr.optim.cg, deepmr.recon.alg.linop) through the same
+    stub parents. The Toeplitz kernel value is converted to numpy right after
+    planning (the CPU path of apply_toeplitz needs it, toeplitz.py:85)."""
+    import_reference()
+    for name, sub in [("deepmr.optim", "/optim"), ("deepmr.recon", "/recon"), ("deepmr.recon.alg", "/recon/alg")]:
+        mod = types.ModuleType(name)
+        mod.__path__ = [REF_SRC + sub]
+        sys.modules[name] = mod
+    fft = sys.modules["deepmr.fft"]
+    plan = fft.plan_toeplitz_nufft
+
+    def plan_fixed(*args, **kwargs):
+        T = plan(*args, **kwargs)
+        T.value = T.value.numpy()
+        return T
+
+    fft.plan_toeplitz_nufft = plan_fixed
+    import deepmr.optim.cg as cg  # noqa: E402
+    import deepmr.recon.alg.linop as enc  # noqa: E402
+
+    return cg, enc
+
+
+def cgsense_case(name="cgsense2d", N=128, ncoils=8, nspokes=96, nsamples=256, niter=20, seed=0):
+    """CG-SENSE of the reference (recon_lstsq with toeplitz=True: EncodingOp +
+    zero-filled AHy + cg_solve, src/deepmr/recon/alg/classic_recon.py:133-174,
+    without the intensity rescaling) on a 2D golden-angle radial acquisition:
+    seeded phantom with a phase ramp, random-phase Gaussian coil maps, ramp
+    density weights, data = E x + complex Gaussian noise. Saves the inputs, the
+    reference's AHy and its solution after `niter` CG iterations (tol = 0)."""
+    cg, enc = import_reference_recon()
+    coord = torch.as_tensor(synth.radial_2d(nspokes, nsamples, N))
+    dcf = torch.as_tensor(synth.ramp_dcf(coord.numpy()))
+    maps = torch.as_tensor(synth.coil_maps(ncoils, (N, N), seed=seed + 5))
+    ph = synth.ellipse_phantom(N, seed=seed + 2)
+    x = torch.as_tensor(ph * np.exp(1j * 0.3 * np.linspace(-1, 1, N))[None, :]).to(torch.complex64)
+    data = torch.zeros((ncoils, 1, nspokes, nsamples), dtype=torch.complex64)
+    E, EHE = enc.EncodingOp(data, traj=coord, dcf=dcf, shape=(N, N), sensmap=maps[None, None],
+                            toeplitz=True, device="cpu")
+    y = E(x[None])[0, 0]  # (ncoils, nspokes, nsamples)
+    g = torch.Generator().manual_seed(seed + 7)
+    sigma = 1e-2 * float(y.abs().pow(2).mean().sqrt())
+    y = y + sigma * torch.complex(torch.randn(y.shape, generator=g), torch.randn(y.shape, generator=g)) * 0.5**0.5
+    y = y.to(torch.complex64)
+    ahy = E.H(dcf**0.5 * y[None, None])  # (1, N, N)
+    out, _ = cg.cg_solve(ahy, EHE, niter=niter, tol=0.0, ndim=2)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"), coord=_np(coord), dcf=_np(dcf), maps=_np(maps), kspace=_np(y),
+        shape=np.int32(N), niter=np.int32(niter), ahy=_np(ahy[0]), x_cg=_np(out[0]),
+    )
+    print("wrote", name)
 
 
 def _np(x):
@@ -211,6 +279,9 @@ def main():
     if sys.argv[1:] == ["lowrank"]:
         lowrank_cases(N)
         return
+    if sys.argv[1:] == ["cgsense"]:
+        cgsense_case()
+        return
     if sys.argv[1:] == ["sparse"]:
         sparse_cases()
         return
@@ -276,6 +347,7 @@ def main():
 
     lowrank_cases(N)
     sparse_cases()
+    cgsense_case()
 
 
 if __name__ == "__main__":

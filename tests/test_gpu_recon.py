@@ -60,6 +60,62 @@ def test_cg_sense_vs_oracle(small_recon):
     assert rel(x, x_ref) < 1e-4, rel(x, x_ref)
 
 
+def test_cg_sense_vs_reference_fixture(load_golden):
+    """CG-SENSE against the reference's own recon pipeline: EncodingOp with
+    toeplitz=True, AHy = E^H(dcf**0.5 y) and cg_solve for 20 iterations
+    (src/deepmr/recon/alg/linop.py:108-148, classic_recon.py:153-174,
+    optim/cg.py:16-221), run by tests/golden/make_golden.py on a 128^2,
+    8-coil, 96 x 256 radial acquisition. Tolerance 1e-5 relative L2 for AHy
+    and for the 20-iteration solution."""
+    from deepmr_b200 import recon
+
+    g = load_golden("cgsense2d")
+    N = int(g["shape"])
+    maps = torch.as_tensor(g["maps"]).cuda()
+    plan = recon._nufft.plan_nufft(torch.as_tensor(g["coord"]), (N, N), 4, 1.25, "cuda")
+    dcf = torch.as_tensor(g["dcf"]).cuda()
+    ahy = recon.sense_adjoint(torch.as_tensor(g["kspace"]).cuda(), plan, maps, dcf)
+    assert rel(ahy, g["ahy"]) < 1e-5, rel(ahy, g["ahy"])
+    x = recon.cg_sense(g["kspace"], g["coord"], (N, N), maps, g["dcf"], niter=int(g["niter"]))
+    e = rel(x, g["x_cg"])
+    print(f"CG-SENSE vs reference: AHy {rel(ahy, g['ahy']):.2e}, 20 iterations {e:.2e}")
+    assert e < 1e-5, e
+
+
+def test_encoding_op_cg_solve_dropin(load_golden):
+    """The reference's CG-SENSE caller code, unchanged, on the drop-in operators:
+    E, EHE = EncodingOp(..., toeplitz=True); AHy = E.H(dcf**0.5 * y);
+    cg_solve(AHy, EHE, niter=20) (src/deepmr/recon/alg/classic_recon.py:133-174).
+    EHE is fused (one dmr_sense_normal per application, CG on the device); the
+    same iteration through the generic torch CG (a plain callable operator)
+    agrees too. Tolerance 1e-5 against the reference's output."""
+    from deepmr_b200 import linops, optim
+
+    g = load_golden("cgsense2d")
+    N = int(g["shape"])
+    maps = torch.as_tensor(g["maps"])
+    coord, dcf = torch.as_tensor(g["coord"]), torch.as_tensor(g["dcf"]).cuda()
+    y = torch.as_tensor(g["kspace"]).cuda()
+    data = torch.zeros((maps.shape[0], 1) + tuple(y.shape[1:]), dtype=torch.complex64, device="cuda")
+    E, EHE = linops.EncodingOp(data, traj=coord, dcf=dcf, shape=(N, N), sensmap=maps[None, None].cuda(),
+                               toeplitz=True, device="cuda")
+    assert EHE.fused is not None
+    img = E.H(dcf**0.5 * y[None, None])
+    assert tuple(img.shape) == (1, N, N)
+    assert rel(img[0], g["ahy"]) < 1e-5, rel(img[0], g["ahy"])
+    out, _ = optim.cg_solve(img, EHE, niter=int(g["niter"]), tol=0.0, ndim=2)
+    assert tuple(out.shape) == (1, N, N) and out.device.type == "cuda"
+    assert rel(out[0], g["x_cg"]) < 1e-5, rel(out[0], g["x_cg"])
+    # generic CG (complex64 inner products, as the reference) over the same operator
+    out2, _ = optim.cg_solve(img, lambda v: EHE(v), niter=int(g["niter"]), tol=0.0, ndim=2)
+    assert rel(out2[0], g["x_cg"]) < 1e-5, rel(out2[0], g["x_cg"])
+    # unfused composition (three operators) gives the same normal operator
+    v = img.clone()
+    unfused = linops.Compose([EHE.linops[0], EHE.linops[1], linops.Identity(2), EHE.linops[2]])
+    assert unfused.fused is None
+    assert rel(unfused(v), EHE(v)) < 1e-5
+
+
 def _requests():
     from deepmr_b200 import recon
 

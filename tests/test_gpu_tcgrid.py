@@ -110,15 +110,64 @@ def test_tc_grid_adjoint_identity(F):
 
 
 def test_tc_grid_no_wait_ran_out(F):
-    """The kernel's bounded mbarrier waits never ran out during these tests."""
+    """The kernel's bounded mbarrier waits do not run out in normal runs."""
     import ctypes
 
     from deepmr_b200 import _lib, synth
 
+    L = _lib.lib()
+    count = ctypes.c_int64(-1)
+    _lib.check(L.dmr_tc_timeouts(ctypes.byref(count), 1))  # reset
     n = 16
     coord = synth.kooshball_3d(200, 2 * n, n).astype(np.float32)
     plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
     _grid(F, plan, synth.complex_gaussian((4,) + coord.shape[:-1], seed=7).cuda())
-    count = ctypes.c_int64(-1)
-    _lib.check(_lib.lib().dmr_tc_timeouts(ctypes.byref(count), 0))
+    plan.interpolator.check_status()
+    _lib.check(L.dmr_tc_timeouts(ctypes.byref(count), 0))
     assert count.value == 0
+
+
+def test_tc_grid_timeout_reported(F):
+    """A bounded wait that runs out is reported, not silent.
+
+    The test hook dmr_tc_test_stall makes every gridding block wait on an
+    mbarrier that nothing signals (bounded by 1 ms of global time): the call
+    returns, dmr_plan_status reports DMR_ERR_TIMEOUT with the number of blocks
+    that stopped, the device counter grows, the Python layer raises on a call
+    whose result returns to the host, and the next normal call is correct."""
+    import ctypes
+
+    from deepmr_b200 import _lib, synth
+
+    L = _lib.lib()
+    n = 16
+    coord = synth.kooshball_3d(200, 2 * n, n).astype(np.float32)
+    plan = F.plan_nufft(torch.as_tensor(coord), n, 4, 1.25, device="cuda")
+    ip = plan.interpolator
+    ksp = synth.complex_gaussian((4,) + coord.shape[:-1], seed=8).cuda()
+    grid = torch.empty((4,) + tuple(ip.dshape), dtype=torch.complex64, device="cuda")
+    st = _lib.stream_ptr(torch.device("cuda", torch.cuda.current_device()))
+    c0, c1 = ctypes.c_int64(-1), ctypes.c_int64(-1)
+    _lib.check(L.dmr_tc_timeouts(ctypes.byref(c0), 0))
+    _lib.check(L.dmr_tc_test_stall(1))
+    try:
+        rc = L.dmr_grid(ip.handle, _lib.ptr(ksp), 0, _lib.ptr(grid), 4, None, 0, 0, st)
+        assert rc == 0  # the launch itself succeeds; the failure is in the status
+        failed = ctypes.c_int32(-1)
+        rc = L.dmr_plan_status(ip.handle, ctypes.byref(failed), 1, st)
+        assert rc == -8, rc  # DMR_ERR_TIMEOUT
+        assert failed.value > 0
+        # the Python layer raises on a call whose result returns to the host
+        with pytest.raises(_lib.DmrError) as ei:
+            F.apply_nufft_adj(ksp.cpu(), plan)
+        assert ei.value.code == -8
+    finally:
+        _lib.check(L.dmr_tc_test_stall(0))
+    _lib.check(L.dmr_tc_timeouts(ctypes.byref(c1), 1))
+    assert c1.value > c0.value
+    # the status was reset by the reads above: a normal call is valid again
+    rc = L.dmr_plan_status(ip.handle, None, 0, st)
+    assert rc == 0
+    x = _grid(F, plan, ksp)
+    ip.check_status()
+    assert rel(x, _grid(F, plan, ksp, det=True)) < TOL

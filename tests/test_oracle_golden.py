@@ -109,3 +109,17 @@ def test_oracle_vs_nudft_small():
     s = np.vdot(y.ravel(), yd.ravel()) / np.vdot(y.ravel(), y.ravel())
     assert abs(abs(s) - 1) < 0.02
     assert R.rel_l2(s * y, yd) < 1e-4
+
+
+@pytest.mark.parametrize("name", golden_cases(kind="cgsense"))
+def test_oracle_cgsense(name, load_golden):
+    """The oracle's CG-SENSE (oracle/cg_ref.py) against the reference's own
+    EncodingOp + cg_solve: AHy to float32 rounding, the 20-iteration solution
+    within 1e-5 (CG steps amplify float32 rounding differences)."""
+    from oracle import cg_ref
+
+    g = load_golden(name)
+    x, ahy, _ = cg_ref.cg_sense(torch.as_tensor(g["kspace"]), g["coord"], int(g["shape"]),
+                                torch.as_tensor(g["maps"]), g["dcf"], int(g["niter"]))
+    assert R.rel_l2(ahy, g["ahy"]) < TOL
+    assert R.rel_l2(x, g["x_cg"]) < 1e-5
