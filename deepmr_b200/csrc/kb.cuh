@@ -27,6 +27,24 @@ __device__ __forceinline__ float kb_f32(float u, float beta)
     return p * expf(a) * rsqrtf(a);
 }
 
+// kb_f32 with both branches of I0 evaluated and one selected (the same
+// arithmetic, no divergence when the lanes of a warp fall on both sides)
+__device__ __forceinline__ float kb_f32_select(float u, float beta)
+{
+    const float a = beta * sqrtf(fmaxf(1.0f - u * u, 0.0f));
+    const float t = a / 3.75f;
+    const float t2 = t * t;
+    const float small = 1.0f + t2 * (3.5156229f + t2 * (3.0899424f + t2 * (1.2067492f
+                        + t2 * (0.2659732f + t2 * (0.0360768f + t2 * 0.0045813f)))));
+    const float v = 3.75f / a;
+    const float p = 0.39894228f + v * (0.01328592f + v * (0.00225319f + v * (-0.00157565f
+                  + v * (0.00916281f + v * (-0.02057706f + v * (0.02635537f
+                  + v * (-0.01647633f + v * 0.00392377f)))))));
+    const float large = p * expf(a) * rsqrtf(a);
+    const float r = a < 3.75f ? small : large;
+    return fabsf(u) > 1.0f ? 0.0f : r;
+}
+
 inline double kb_f64(double u, double beta)
 {
     if (fabs(u) > 1.0) return 0.0;

@@ -116,12 +116,72 @@ __global__ void gather_sorted_kernel(int64_t total, int ndim, const int32_t *__r
     }
 }
 
-// sort key (frame, bin, cell) -> (frame, bin)
-__global__ void bin_key_kernel(int64_t total, int cells, int32_t *__restrict__ keys)
+// sort key of the tensor-core gridding bins: (frame, bin) with tile tg_T
+__global__ void tg_key_kernel(Geom g, int t0, int t1, int t2, int n0, int n1, int n2, int nbins,
+                              const int64_t *__restrict__ foff, const float *__restrict__ rk0,
+                              const float *__restrict__ rk1, const float *__restrict__ rk2,
+                              int32_t *__restrict__ keys, int32_t *__restrict__ counts)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x)
-        keys[i] /= cells;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int lo = 0, hi = g.nframes;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (foff[mid] <= i) lo = mid; else hi = mid;
+        }
+        const int bx = pmod(first_tap(rk0[i], g.W[0]), g.G[0]) / t0;
+        const int by = pmod(first_tap(rk1[i], g.W[1]), g.G[1]) / t1;
+        const int bz = pmod(first_tap(rk2[i], g.W[2]), g.G[2]) / t2;
+        const int key = lo * nbins + (bz * n1 + by) * n0 + bx;
+        keys[i] = key;
+        atomicAdd(&counts[key], 1);
+    }
+}
+
+// Per sample of the tensor-core gridding order: the Kaiser-Bessel weights of
+// its W taps on each axis (the same arithmetic as tap_weight in the kernels)
+// and the offsets of its first taps inside its bin (tile t).
+__global__ void tg_weights_kernel(Geom g, int t0, int t1, int t2, int wp, const float *__restrict__ sc0,
+                                  const float *__restrict__ sc1, const float *__restrict__ sc2,
+                                  float *__restrict__ w, int32_t *__restrict__ l)
+{
+    const int tt[3] = {t0, t1, t2};
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < g.total;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const float k[3] = {sc0[j], sc1[j], sc2[j]};
+        int pack = 0;
+        for (int a = 0; a < 3; a++) {
+            const int x0 = first_tap(k[a], g.W[a]);
+            pack |= (pmod(x0, g.G[a]) % tt[a]) << (8 * a);
+            for (int i = 0; i < wp; i++)
+                w[(j * 3 + a) * wp + i] = i < g.W[a] ? tap_weight(x0, i, k[a], g.W[a], g.inv_hw[a], g.beta[a]) : 0.0f;
+        }
+        l[j] = pack;
+    }
+}
+
+// Work items of at most `chunk` samples per non-empty bin, and their visiting
+// order in 4 x 4 x 4-bin tiles (frame, tile z, y, x, bin z, y, x), so that
+// bins sharing halo points or spokes run close together.
+static void make_items(const std::vector<int32_t> &start, int nbins, const int nb[3], int chunk,
+                       std::vector<WorkItem> &items, std::vector<int32_t> &order)
+{
+    items.clear();
+    const int64_t nkeys = (int64_t)start.size() - 1;
+    for (int64_t b = 0; b < nkeys; b++)
+        for (int s = start[b]; s < start[b + 1]; s += chunk)
+            items.push_back({(int)b, s, std::min(s + chunk, start[b + 1])});
+    order.resize(items.size());
+    for (size_t i = 0; i < items.size(); i++) order[i] = (int32_t)i;
+    auto tkey = [&](const WorkItem &w) {
+        const int64_t f = w.bin / nbins, lb = w.bin % nbins;
+        const int64_t bx = lb % nb[0], by = (lb / nb[0]) % nb[1], bz = lb / ((int64_t)nb[0] * nb[1]);
+        const int64_t ntx = (nb[0] + 3) >> 2, nty = (nb[1] + 3) >> 2, ntz = (nb[2] + 3) >> 2;
+        const int64_t tile = ((f * ntz + (bz >> 2)) * nty + (by >> 2)) * ntx + (bx >> 2);
+        return tile * 64 + (((bz & 3) * 4 + (by & 3)) * 4 + (bx & 3));
+    };
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return tkey(items[a]) < tkey(items[b]); });
 }
 
 static int grid_blocks(int64_t n, int threads)
@@ -392,34 +452,7 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
         gather_sorted_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
             total, ndim, p->sidx, rk[0], rk[1], rk[2], p->scoord[0], p->scoord[1], p->scoord[2]);
         DMR_LAUNCHED("gather_sorted_kernel");
-        // 3D: the same bins in acquisition order (stable sort by (frame, bin) alone)
-        if (ndim == 3 && cell_order) {
-            const int cells = g.T[0] * g.T[1] * g.T[2];
-            bin_key_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(total, cells, keys);
-            DMR_LAUNCHED("bin_key_kernel");
-            int bin_bit = 1;
-            while ((1ll << bin_bit) < nkeys) bin_bit++;
-            for (int a = 0; a < 3; a++) DMR_TRY(dev_alloc(&p->acq_scoord[a], total));
-            DMR_TRY(dev_alloc(&p->acq_sidx, total));
-            p->acq_owned = true;
-            size_t tb2 = 0;
-            DMR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, keys, keys_s, vals, p->acq_sidx,
-                                                     (int)total, 0, bin_bit, st));
-            DMR_CHECK(tb2 <= std::max<size_t>(temp_bytes, 1), DMR_ERR_INVALID, "sort scratch");
-            DMR_CUDA(cub::DeviceRadixSort::SortPairs(temp, tb2, keys, keys_s, vals, p->acq_sidx,
-                                                     (int)total, 0, bin_bit, st));
-            g_launches.fetch_add(1);
-            gather_sorted_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
-                total, ndim, p->acq_sidx, rk[0], rk[1], rk[2], p->acq_scoord[0], p->acq_scoord[1],
-                p->acq_scoord[2]);
-            DMR_LAUNCHED("gather_sorted_kernel");
-        }
     }
-    if (!p->acq_owned) {
-        for (int a = 0; a < 3; a++) p->acq_scoord[a] = p->scoord[a];
-        p->acq_sidx = p->sidx;
-    }
-
     std::vector<int32_t> h_counts(nkeys);
     int h_err = 0;
     DMR_CUDA(cudaMemcpyAsync(h_counts.data(), counts, nkeys * sizeof(int32_t),
@@ -431,6 +464,74 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
     // bin offsets
     std::vector<int32_t> h_start(nkeys + 1, 0);
     for (int64_t i = 0; i < nkeys; i++) h_start[i + 1] = h_start[i] + h_counts[i];
+
+    // bins of the 3D tensor-core gridding: region (T + W - 1) of 7 x 6 x 6
+    // points (x, y, z), i.e. T = (8 - W, 7 - W, 7 - W), for widths 2..5
+    if (ndim == 3 && total > 0 && g.W[0] == g.W[1] && g.W[1] == g.W[2] && g.W[0] >= 2 && g.W[0] <= 5) {
+        const int W = g.W[0];
+        int tT[3] = {8 - W, 7 - W, 7 - W}, tnb[3];
+        for (int a = 0; a < 3; a++) {
+            tT[a] = std::min(tT[a], g.G[a]);
+            tnb[a] = (int)ceil_div(g.G[a], tT[a]);
+        }
+        const int tbins = tnb[0] * tnb[1] * tnb[2];
+        const int64_t tkeys = (int64_t)nframes * tbins;
+        if (tkeys < INT32_MAX) {
+            int32_t *tcounts = nullptr;
+            DMR_TRY(dev_alloc(&tcounts, tkeys));
+            tmp.ptr[10] = tcounts;
+            DMR_CUDA(cudaMemsetAsync(tcounts, 0, tkeys * sizeof(int32_t), st));
+            tg_key_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(g, tT[0], tT[1], tT[2], tnb[0], tnb[1], tnb[2],
+                                                                   tbins, d_foff, rk[0], rk[1], rk[2], keys, tcounts);
+            DMR_LAUNCHED("tg_key_kernel");
+            int tbit = 1;
+            while ((1ll << tbit) < tkeys) tbit++;
+            for (int a = 0; a < 3; a++) DMR_TRY(dev_alloc(&p->tg_scoord[a], total));
+            DMR_TRY(dev_alloc(&p->tg_sidx, total));
+            size_t tb = 0;
+            DMR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys_s, vals, p->tg_sidx, (int)total, 0,
+                                                     tbit, st));
+            void *ttemp = nullptr;
+            DMR_CUDA(cudaMalloc(&ttemp, std::max<size_t>(tb, 1)));
+            tmp.ptr[11] = ttemp;
+            DMR_CUDA(cub::DeviceRadixSort::SortPairs(ttemp, tb, keys, keys_s, vals, p->tg_sidx, (int)total, 0,
+                                                     tbit, st));
+            g_launches.fetch_add(1);
+            gather_sorted_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(
+                total, ndim, p->tg_sidx, rk[0], rk[1], rk[2], p->tg_scoord[0], p->tg_scoord[1], p->tg_scoord[2]);
+            DMR_LAUNCHED("gather_sorted_kernel");
+            p->tg_wp = W <= 4 ? 4 : 8;
+            DMR_TRY(dev_alloc(&p->tg_w, (size_t)total * 3 * p->tg_wp));
+            DMR_TRY(dev_alloc(&p->tg_l, total));
+            tg_weights_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(g, tT[0], tT[1], tT[2], p->tg_wp,
+                                                                       p->tg_scoord[0], p->tg_scoord[1],
+                                                                       p->tg_scoord[2], p->tg_w, p->tg_l);
+            DMR_LAUNCHED("tg_weights_kernel");
+            std::vector<int32_t> hc(tkeys);
+            DMR_CUDA(cudaMemcpyAsync(hc.data(), tcounts, tkeys * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            DMR_CUDA(cudaStreamSynchronize(st));
+            std::vector<int32_t> ts(tkeys + 1, 0);
+            for (int64_t i = 0; i < tkeys; i++) ts[i + 1] = ts[i] + hc[i];
+            std::vector<WorkItem> titems;
+            std::vector<int32_t> torder;
+            make_items(ts, tbins, tnb, 2048, titems, torder);
+            DMR_TRY(dev_alloc(&p->tg_work, titems.size()));
+            DMR_TRY(dev_alloc(&p->tg_order, torder.size()));
+            if (!titems.empty()) {
+                DMR_CUDA(cudaMemcpyAsync(p->tg_work, titems.data(), titems.size() * sizeof(WorkItem),
+                                         cudaMemcpyHostToDevice, st));
+                DMR_CUDA(cudaMemcpyAsync(p->tg_order, torder.data(), torder.size() * sizeof(int32_t),
+                                         cudaMemcpyHostToDevice, st));
+            }
+            DMR_CUDA(cudaStreamSynchronize(st));
+            p->tg_nwork = (int)titems.size();
+            p->tg_nbins = tbins;
+            for (int a = 0; a < 3; a++) {
+                p->tg_T[a] = tT[a];
+                p->tg_nb[a] = tnb[a];
+            }
+        }
+    }
 
     // interpolation / atomic-gridding items: non-empty bins in chunks of at most
     // kChunk samples (bounded work per block), in spatial order so that blocks

@@ -89,12 +89,26 @@ struct dmr_plan {
     // device buffers
     float *scoord[3] = {nullptr, nullptr, nullptr};  // sorted rescaled coordinates
     int32_t *sidx = nullptr;            // sorted position -> global sample index
-    // 3D plans: the same bins with their samples in acquisition order (the
-    // tensor-core gridding reads consecutive samples of a spoke together);
-    // alias scoord / sidx when the plan's own order already is that
-    float *acq_scoord[3] = {nullptr, nullptr, nullptr};
-    int32_t *acq_sidx = nullptr;
-    bool acq_owned = false;
+    // 3D tensor-core gridding: bins of its own (tile tg_T, x y z) whose region
+    // (tile + W - 1 per axis) is at most 7 x 6 x 6 = 252 points, one N = 256
+    // MMA; the samples of a bin in acquisition order (consecutive samples of a
+    // spoke, which share 32-byte sectors of k-space, are read together);
+    // work items of at most 2048 samples, visited in 4 x 4 x 4-bin tiles.
+    // tg_T[0] == 0: not planned.
+    int tg_T[3] = {0, 0, 0};
+    int tg_nb[3] = {1, 1, 1};
+    int tg_nbins = 0;
+    float *tg_scoord[3] = {nullptr, nullptr, nullptr};
+    int32_t *tg_sidx = nullptr;
+    // per sample (gridding order): the Kaiser-Bessel weights of its W taps on
+    // each axis, [sample][axis][tg_wp] (tg_wp = 4 for W <= 4, else 8), and the
+    // offsets of its first taps inside its bin, x | y << 8 | z << 16
+    float *tg_w = nullptr;
+    int32_t *tg_l = nullptr;
+    int tg_wp = 0;
+    dmr::WorkItem *tg_work = nullptr;
+    int tg_nwork = 0;
+    int32_t *tg_order = nullptr;
     int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
     dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
     int nwork = 0;
@@ -125,10 +139,12 @@ struct dmr_plan {
             cudaFree(apod[a]);
         }
         cudaFree(sidx);
-        if (acq_owned) {
-            for (int a = 0; a < 3; a++) cudaFree(acq_scoord[a]);
-            cudaFree(acq_sidx);
-        }
+        for (int a = 0; a < 3; a++) cudaFree(tg_scoord[a]);
+        cudaFree(tg_sidx);
+        cudaFree(tg_w);
+        cudaFree(tg_l);
+        cudaFree(tg_work);
+        cudaFree(tg_order);
         cudaFree(bin_start);
         cudaFree(work);
         cudaFree(work_order);
