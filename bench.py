@@ -35,11 +35,10 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(N=192, coils=32, spokes=50000, samples=384, width=4, oversamp=1.25)
 FALLBACK_HBM_GBS = 6650.0
 METRIC = "NUFFT fwd+adj k-space samples/s (3D kooshball)"
-# kernels the library launches for 3D, width 4, 32 coils (spread.cu dispatch)
 # kernels that run the workload's interpolation / gridding (3D, width 4, 32 coils):
-# tensor-core gridding unless DMR_NO_TC selects the cell-cube kernel
+# tensor-core gridding (grid_tmem_kernel) unless DMR_NO_TC selects the cell-cube kernel
 KERNELS = {"interp": "interp_cube_kernel",
-           "grid": "grid_cube_kernel" if os.environ.get("DMR_NO_TC", "0") not in ("", "0") else "grid_tc_kernel",
+           "grid": "grid_cube_kernel" if os.environ.get("DMR_NO_TC", "0") not in ("", "0") else "grid_tmem_kernel",
            "grid_det": "grid_rt_kernel"}
 UNIT = "samples/s"
 
