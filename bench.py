@@ -39,7 +39,7 @@ METRIC = "NUFFT fwd+adj k-space samples/s (3D kooshball)"
 # tensor-core gridding (grid_tmem_kernel) unless DMR_NO_TC selects the cell-cube kernel
 KERNELS = {"interp": "interp_cube_kernel",
            "grid": "grid_cube_kernel" if os.environ.get("DMR_NO_TC", "0") not in ("", "0") else "grid_tmem_kernel",
-           "grid_det": "grid_rt_kernel"}
+           "grid_det": "grid_tmem_kernel"}
 UNIT = "samples/s"
 
 

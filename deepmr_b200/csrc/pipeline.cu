@@ -189,7 +189,7 @@ static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, Nufft
     if (!fp) return err;
     const size_t grid_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
     const size_t fft_bytes = align_up(fp->work_bytes, 256);
-    const size_t rt_bytes = align_up(rt_scratch_bytes(p, batch), 256);
+    const size_t rt_bytes = align_up(grid_scratch_bytes(p, batch), 256);
     const size_t total = grid_bytes + fft_bytes + rt_bytes;
     if (need) *need = total;
     if (!ws) return DMR_OK;
@@ -524,7 +524,7 @@ static int lowrank_ws(dmr_plan *p, int64_t batch, int64_t ncoeff, void *ws, size
     const size_t coef_bytes = align_up((size_t)batch * ncoeff * g.gsize * sizeof(float2), 256);
     const size_t frame_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
     const size_t fft_bytes = align_up(fp->work_bytes, 256);
-    const size_t rt_bytes = align_up(rt_scratch_bytes(p, batch), 256);
+    const size_t rt_bytes = align_up(grid_scratch_bytes(p, batch), 256);
     const size_t total = coef_bytes + frame_bytes + fft_bytes + rt_bytes;
     if (need) *need = total;
     if (!ws) return DMR_OK;

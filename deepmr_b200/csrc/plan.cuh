@@ -41,6 +41,11 @@ struct WorkItem {
     int end;
 };
 
+// Samples of a tensor-core gridding work item, at most: the MMA's fp32 sums in
+// tensor memory lose accuracy over longer chains, and longer items would
+// unbalance the blocks.
+constexpr int kTgSegment = 2048;
+
 // One block of register-tile gridding: part `begin` of `end` equal fractions
 // of every window bin of block region `region` (frame included). slot < 0:
 // the block writes the grid; otherwise it writes partial sums to scratch slot
@@ -69,14 +74,24 @@ std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t bat
 bool rt_geometry_ok(const Geom &g);
 int rt_build(::dmr_plan *p, const std::vector<int32_t> &h_start, cudaStream_t st);
 size_t rt_scratch_bytes(const ::dmr_plan *p, int64_t batch);
+// scratch bytes of deterministic tensor-core gridding (split bins' partial sums)
+size_t tm_scratch_bytes(const ::dmr_plan *p, int64_t batch);
+// scratch bytes a gridding call of `batch` coils may need (either kernel)
+size_t grid_scratch_bytes(const ::dmr_plan *p, int64_t batch);
+// library-owned stream-ordered pool for the scratch of calls without a workspace
+cudaMemPool_t scratch_pool(int dev);
 // tensor-core atomic gridding of 3D plans (tcgrid.cu); DMR_ERR_UNSUPPORTED when
 // the bin region does not fit
 int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                     const float *weight, int wpb, cudaStream_t st);
-// the same with the spreading operand in tensor memory (tmgrid.cu); `timeouts`
-// is the device address of the process-wide counter of blocks that stopped
+                     const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
+                     cudaStream_t st);
+// tensor-core gridding with the plan's gridding bins (tmgrid.cu), atomic or
+// deterministic (colour launches; scratch from the caller when it holds
+// tm_scratch_bytes, else from the library pool); `timeouts` is the device
+// address of the process-wide counter of blocks that stopped on a bounded wait
 int grid_tm_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                     const float *weight, int wpb, int *timeouts, int stall, cudaStream_t st);
+                     const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes, int *timeouts,
+                     int stall, cudaStream_t st);
 
 }  // namespace dmr
 
@@ -109,6 +124,20 @@ struct dmr_plan {
     dmr::WorkItem *tg_work = nullptr;
     int tg_nwork = 0;
     int32_t *tg_order = nullptr;
+    // deterministic mode: bins grouped by colour (bins of one colour have
+    // disjoint regions; colours run in order), heaviest first within a colour.
+    // A bin of more than dmr::kTgSegment samples is split into segments of that
+    // many, which run in parallel and write partial sums to scratch slot
+    // tg_det_slot[item] (-1: the item adds into the grid, the only addition to
+    // its points in the colour); the colour's reduction items (bin, first slot,
+    // end slot) then add the slots of each split bin in slot order.
+    dmr::WorkItem *tg_det_work = nullptr;
+    int32_t *tg_det_slot = nullptr;
+    dmr::WorkItem *tg_det_red = nullptr;
+    int32_t *tg_iota = nullptr;          // 0, 1, 2, ... (identity visiting order)
+    std::vector<int> tg_det_cstart;      // host, ncolours + 1 (items)
+    std::vector<int> tg_det_rstart;      // host, ncolours + 1 (reduction items)
+    int tg_det_slots = 0;                // scratch slots of one colour, at most
     int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
     dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
     int nwork = 0;
@@ -145,6 +174,10 @@ struct dmr_plan {
         cudaFree(tg_l);
         cudaFree(tg_work);
         cudaFree(tg_order);
+        cudaFree(tg_det_work);
+        cudaFree(tg_det_slot);
+        cudaFree(tg_det_red);
+        cudaFree(tg_iota);
         cudaFree(bin_start);
         cudaFree(work);
         cudaFree(work_order);

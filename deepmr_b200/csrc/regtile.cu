@@ -598,7 +598,7 @@ size_t rt_scratch_bytes(const dmr_plan *p, int64_t batch)
 }
 
 // Library-owned stream-ordered pool for the scratch of calls without a workspace.
-static cudaMemPool_t rt_pool(int dev)
+cudaMemPool_t scratch_pool(int dev)
 {
     static std::mutex mu;
     static std::map<int, cudaMemPool_t> pools;
@@ -644,7 +644,7 @@ int grid_rt_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     const size_t need = rt_scratch_bytes(p, batch);
     void *owned = nullptr;
     if (need > 0 && (scratch == nullptr || scratch_bytes < need)) {
-        cudaMemPool_t pool = rt_pool(p->device);
+        cudaMemPool_t pool = scratch_pool(p->device);
         if (!pool || cudaMallocFromPoolAsync(&owned, need, pool, st) != cudaSuccess) {
             cudaGetLastError();
             return DMR_ERR_UNSUPPORTED;

@@ -1385,19 +1385,25 @@ int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t 
 int grid_rt_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, void *scratch, size_t scratch_bytes, cudaStream_t st);
 
+size_t grid_scratch_bytes(const dmr_plan *p, int64_t batch)
+{
+    return std::max(rt_scratch_bytes(p, batch), tm_scratch_bytes(p, batch));
+}
+
 int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                   const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
                   cudaStream_t st)
 {
-    // deterministic 3D gridding of 8+ coils: register tiles (one owner per grid
-    // point, no colour passes) when the plan has them
-    if (det) {
-        const int rc = grid_rt_dispatch(p, ksp, kreal, grid, batch, weight, wpb, scratch, scratch_bytes, st);
+    // 3D gridding on the tensor cores: atomic, or deterministic in colour
+    // launches (bitwise reproducible), when the plan's gridding bins apply
+    if (p->g.ndim == 3 && grid_variant() == 0) {
+        const int rc = grid_tc_dispatch(p, ksp, kreal, grid, batch, weight, wpb, det, scratch, scratch_bytes, st);
         if (rc != DMR_ERR_UNSUPPORTED) return rc;
     }
-    // atomic 3D gridding: tensor-core spreading when the bin region fits
-    if (!det && p->g.ndim == 3 && grid_variant() == 0) {
-        const int rc = grid_tc_dispatch(p, ksp, kreal, grid, batch, weight, wpb, st);
+    // deterministic 3D gridding of 8+ coils otherwise: register tiles (one owner
+    // per grid point, no colour passes) when the plan has them
+    if (det) {
+        const int rc = grid_rt_dispatch(p, ksp, kreal, grid, batch, weight, wpb, scratch, scratch_bytes, st);
         if (rc != DMR_ERR_UNSUPPORTED) return rc;
     }
     const int cw = cube_width(p->g);

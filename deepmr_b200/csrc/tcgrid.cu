@@ -429,10 +429,13 @@ static bool tc_shape(const Geom &g, int64_t batch, TcShape &s)
     return s.ncols <= 512;
 }
 
-// Tensor-core gridding of a 3D plan (atomic accumulation); DMR_ERR_UNSUPPORTED
-// when the geometry does not fit (then the caller uses the cell-cube kernels).
+// Tensor-core gridding of a 3D plan: the kernel of tmgrid.cu (atomic, or
+// deterministic in colour launches), else, in atomic mode, the kernel above;
+// DMR_ERR_UNSUPPORTED when neither applies (then the caller uses the
+// CUDA-core kernels).
 int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                     const float *weight, int wpb, cudaStream_t st)
+                     const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
+                     cudaStream_t st)
 {
     if (tc_disabled()) return DMR_ERR_UNSUPPORTED;
     int dev = 0;
@@ -440,9 +443,12 @@ int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     if (!tm_disabled()) {
         int *timeouts = nullptr;
         DMR_TRY(timeouts_ptr(dev, &timeouts));
-        const int rc = grid_tm_dispatch(p, ksp, kreal, grid, batch, weight, wpb, timeouts, g_tc_stall.load(), st);
+        const int rc =
+            grid_tm_dispatch(p, ksp, kreal, grid, batch, weight, wpb, det, scratch, scratch_bytes, timeouts,
+                             g_tc_stall.load(), st);
         if (rc != DMR_ERR_UNSUPPORTED) return rc;
     }
+    if (det) return DMR_ERR_UNSUPPORTED;  // the kernel above adds with atomics in any order
     TcShape sh;
     if (!tc_shape(p->g, batch, sh)) return DMR_ERR_UNSUPPORTED;
     int sms = 0, smem_sm = 0, smem_blk = 0, reserved = 0;

@@ -69,6 +69,11 @@ constexpr int kTmMaxRows = 24;             // region rows over the three axes (7
 constexpr int kTmTable = kTmMaxRows * 8;   // a chunk's weight table: rows x 8 samples
 constexpr int kTmSC = 8;                   // samples per chunk (K of one tf32 MMA)
 constexpr int kTmSB = 128;                 // samples per pass
+// samples accumulated in tensor memory before a read-back: the fp32 sums of
+// the MMA lose accuracy over long chains, so a longer work item is read back
+// in segments of this many samples (a multiple of kTmSB)
+constexpr int kTmSeg = kTgSegment;
+static_assert(kTmSeg % kTmSB == 0, "segments of whole passes");
 constexpr int kTmSBP = kTmSB + 4;          // padded row (bank spread)
 constexpr int kTmMaxSlots = 3;             // pass ring
 constexpr int kTmMaxStages = 4;            // operand stages
@@ -234,6 +239,11 @@ struct PassSeq {
         base += kTmSB;
         if (base >= it.end) next_task(work, order);
     }
+    __device__ void next_segment(const WorkItem *work, const int32_t *order)
+    {
+        base += kTmSeg;
+        if (base >= it.end) next_task(work, order);
+    }
 };
 
 __device__ __forceinline__ void bin_origin(const Geom &g, int bin, int &f, int org[3])
@@ -249,8 +259,8 @@ __device__ __forceinline__ void bin_origin(const Geom &g, int bin, int &f, int o
 __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
     Geom g, TmShape sh, const WorkItem *__restrict__ work, const int32_t *__restrict__ order, int nwork,
     int nchunks, const float *__restrict__ tw, const int32_t *__restrict__ tl, const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid,
-    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale, int *__restrict__ status,
-    int *__restrict__ timeouts, int stall)
+    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale, const int32_t *__restrict__ dslot,
+    float2 *__restrict__ scratch, int *__restrict__ status, int *__restrict__ timeouts, int stall)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[kBarCount];
@@ -478,6 +488,10 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                 goff[et] = (gz * g.G[1] + gy) * g.G[0] + gx;
             }
             const float2 *gitem = grid + (b0 * g.nframes + f) * g.gsize;
+            // a segment of a split bin (deterministic mode) stores its partial
+            // sums into its scratch slot, [coil][region point]
+            const int dsl = dslot ? dslot[order[ps.task / nchunks]] : -1;
+            float2 *part = dsl >= 0 ? scratch + ((int64_t)dsl * nchunks + ps.task % nchunks) * sh.CC * kTmN : nullptr;
             const int64_t cstride = (int64_t)g.nframes * g.gsize;
             uint32_t r[16], rn[16];
             tc_ld16(tbase + lanebase + (uint32_t)(acc * kTmN + 16 * hcol), r);
@@ -506,11 +520,19 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                                             (xb[(2 * c + 1) * kTmXS + lane] + xb[(65 + 2 * c) * kTmXS + lane]) *
                                                 inv_scale);
                     }
+                    if (part) {
 #pragma unroll
-                    for (int cc = 0; cc < 4; cc++) {
-                        const int c = e * 4 + cc;
-                        if (c < cact && (v[cc].x != 0.0f || v[cc].y != 0.0f))
-                            atomicAdd(const_cast<float2 *>(gp) + c * cstride, v[cc]);
+                        for (int cc = 0; cc < 4; cc++) {
+                            const int c = e * 4 + cc;
+                            if (c < cact) part[c * kTmN + pp] = v[cc];
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < 4; cc++) {
+                            const int c = e * 4 + cc;
+                            if (c < cact && (v[cc].x != 0.0f || v[cc].y != 0.0f))
+                                atomicAdd(const_cast<float2 *>(gp) + c * cstride, v[cc]);
+                        }
                     }
                 }
                 if (more) {
@@ -521,7 +543,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             bar_arrive(bar_addr(bars, kBarAccEmpty + acc));
-            ps.next_task(work, order);
+            ps.next_segment(work, order);
         }
     } else if (warp == kTmMmaWarp) {
         // ------------------------------------------------------------------ MMA issue
@@ -593,7 +615,8 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             if (lane == 0) {
                 int *meta = reinterpret_cast<int *>(sl + sh.meta_off);
                 meta[0] = it.bin;
-                meta[1] = (base == it.begin ? kPassFirst : 0) | (base + kTmSB >= it.end ? kPassLast : 0);
+                meta[1] = ((base - it.begin) % kTmSeg == 0 ? kPassFirst : 0) |
+                          (base + kTmSB >= it.end || (base + kTmSB - it.begin) % kTmSeg == 0 ? kPassLast : 0);
                 meta[2] = n;
                 meta[3] = (int)b0;
                 meta[4] = cact;
@@ -667,6 +690,43 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
     }
 }
 
+// Deterministic mode: the split bins of one colour (reduction items: bin,
+// first slot, end slot) add their segments' partial sums, in slot order, into
+// the grid; one block per (item, coil block), thread = (coil, region point).
+// No other block of the launch touches the bin's region points.
+__global__ void __launch_bounds__(256) grid_tm_reduce_kernel(Geom g, TmShape sh, const WorkItem *__restrict__ red,
+                                                            const float2 *__restrict__ scratch, float2 *grid,
+                                                            int64_t batch, int nchunks)
+{
+    const WorkItem r = red[blockIdx.x];
+    const int cch = blockIdx.y;
+    int f, org[3];
+    bin_origin(g, r.bin, f, org);
+    const int64_t b0 = (int64_t)cch * sh.CC;
+    const int cact = (int)(batch - b0 < (int64_t)sh.CC ? batch - b0 : (int64_t)sh.CC);
+    const int RXY = sh.R[0] * sh.R[1];
+    const int64_t sstride = (int64_t)nchunks * sh.CC * kTmN;
+    const float2 *src = scratch + ((int64_t)r.begin * nchunks + cch) * sh.CC * kTmN;
+    for (int e = threadIdx.x; e < cact * kTmN; e += blockDim.x) {
+        const int c = e / kTmN, pt = e - c * kTmN;
+        if (pt >= sh.P) continue;
+        float2 acc = make_float2(0.0f, 0.0f);
+        for (int s = 0; s < r.end - r.begin; s++) {
+            const float2 v = src[s * sstride + e];
+            acc.x += v.x;
+            acc.y += v.y;
+        }
+        const int pz = pt / RXY, pr = pt - pz * RXY;
+        const int py = pr / sh.R[0], px = pr - py * sh.R[0];
+        const int gx = (org[0] + px + g.G[0] - g.half[0]) % g.G[0];
+        const int gy = (org[1] + py + g.G[1] - g.half[1]) % g.G[1];
+        const int gz = (org[2] + pz + g.G[2] - g.half[2]) % g.G[2];
+        float2 *gp = grid + ((b0 + c) * g.nframes + f) * g.gsize + (gz * g.G[1] + gy) * g.G[0] + gx;
+        const float2 o = *gp;
+        *gp = make_float2(o.x + acc.x, o.y + acc.y);
+    }
+}
+
 bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape &s)
 {
     const Geom &g = p->g;
@@ -716,8 +776,16 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
 // Tensor-core gridding of a 3D plan with its gridding bins; DMR_ERR_UNSUPPORTED
 // when the plan has none or the geometry does not fit (the caller then uses
 // the other kernels).
+size_t tm_scratch_bytes(const dmr_plan *p, int64_t batch)
+{
+    if (p->g.ndim != 3 || p->tg_T[0] == 0 || p->tg_det_slots == 0 || batch < 1) return 0;
+    const int64_t cc = std::min<int64_t>(batch, kTmCC);
+    return (size_t)p->tg_det_slots * ceil_div(batch, cc) * cc * kTmN * sizeof(float2);
+}
+
 int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
-                     const float *weight, int wpb, int *timeouts, int stall, cudaStream_t st)
+                     const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes, int *timeouts,
+                     int stall, cudaStream_t st)
 {
     int dev = 0, sms = 0, smem_blk = 0;
     DMR_CUDA(cudaGetDevice(&dev));
@@ -733,11 +801,14 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     int per_sm = 0;
     DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tmem_kernel, kTmThreads, smem));
     if (per_sm != 1) return DMR_ERR_UNSUPPORTED;
+    // deterministic mode needs the points of one region on distinct grid points
+    if (det)
+        for (int a = 0; a < 3; a++)
+            if (sh.R[a] > p->g.G[a]) return DMR_ERR_UNSUPPORTED;
     DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->tg_nwork == 0) return DMR_OK;
     const int64_t nchunks = ceil_div(batch, sh.CC);
-    const int64_t tasks = (int64_t)p->tg_nwork * nchunks;
-    DMR_CHECK(tasks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
+    DMR_CHECK((int64_t)p->tg_nwork * nchunks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
     DMR_CHECK(nchunks * sh.CC < (1ll << 31), DMR_ERR_UNSUPPORTED, "batch too large");
     Geom g = p->g;
     for (int a = 0; a < 3; a++) {
@@ -745,12 +816,53 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
         g.nb[a] = p->tg_nb[a];
     }
     g.nbins = p->tg_nbins;
-    const int blocks = (int)std::min<int64_t>(tasks, (int64_t)sms);
-    grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
-        g, sh, p->tg_work, p->tg_order, p->tg_nwork, (int)nchunks, p->tg_w, p->tg_l, p->tg_sidx, ksp, kreal, grid, batch, weight, wpb, (float)(1.0 / p->scale), p->status,
-        timeouts, stall);
-    DMR_LAUNCHED("grid_tmem_kernel");
-    return DMR_OK;
+    const float inv_scale = (float)(1.0 / p->scale);
+    if (!det) {
+        const int blocks = (int)std::min<int64_t>((int64_t)p->tg_nwork * nchunks, (int64_t)sms);
+        grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
+            g, sh, p->tg_work, p->tg_order, p->tg_nwork, (int)nchunks, p->tg_w, p->tg_l, p->tg_sidx, ksp, kreal,
+            grid, batch, weight, wpb, inv_scale, nullptr, nullptr, p->status, timeouts, stall);
+        DMR_LAUNCHED("grid_tmem_kernel");
+        return DMR_OK;
+    }
+    // deterministic: one launch per colour; within a launch no two bins touch
+    // the same grid point, a whole bin adds into the grid once and a split
+    // bin's segments write scratch slots that the colour's reduction adds in
+    // slot order; the launches run in order on the stream, so every grid point
+    // is summed in the same order in every run
+    const size_t need = tm_scratch_bytes(p, batch);
+    void *owned = nullptr;
+    if (need > 0 && (scratch == nullptr || scratch_bytes < need)) {
+        cudaMemPool_t pool = scratch_pool(p->device);
+        DMR_CHECK(pool != nullptr, DMR_ERR_CUDA, "no memory pool for the gridding scratch");
+        DMR_CUDA(cudaMallocFromPoolAsync(&owned, need, pool, st));
+        scratch = owned;
+    }
+    int rc = DMR_OK;
+    for (size_t c = 0; c + 1 < p->tg_det_cstart.size() && rc == DMR_OK; c++) {
+        const int n = p->tg_det_cstart[c + 1] - p->tg_det_cstart[c];
+        if (n == 0) continue;
+        const int blocks = (int)std::min<int64_t>((int64_t)n * nchunks, (int64_t)sms);
+        grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
+            g, sh, p->tg_det_work + p->tg_det_cstart[c], p->tg_iota, n, (int)nchunks, p->tg_w, p->tg_l,
+            p->tg_sidx, ksp, kreal, grid, batch, weight, wpb, inv_scale, p->tg_det_slot + p->tg_det_cstart[c],
+            (float2 *)scratch, p->status, timeouts, stall);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            rc = cuda_fail(e, "grid_tmem_kernel", __FILE__, __LINE__);
+            break;
+        }
+        const int nr = p->tg_det_rstart[c + 1] - p->tg_det_rstart[c];
+        if (nr == 0) continue;
+        grid_tm_reduce_kernel<<<dim3(nr, (unsigned)nchunks), 256, 0, st>>>(
+            g, sh, p->tg_det_red + p->tg_det_rstart[c], (const float2 *)scratch, grid, batch, (int)nchunks);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "grid_tm_reduce_kernel", __FILE__, __LINE__);
+    }
+    if (owned) cudaFreeAsync(owned, st);
+    return rc;
 }
 
 }  // namespace dmr

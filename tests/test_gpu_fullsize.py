@@ -7,7 +7,9 @@ oversampling 1.25, 32 coils on the GPU. Coils are independent, so coils 0 and
 coils alone (the oracle restates the reference's CPU loops,
 src/deepmr/fft/_interp/interp.py:124-227 and grid.py:181-284). Checked: the
 forward (interpolation), the atomic adjoint (tensor-core gridding) and the
-deterministic adjoint (register-tile gridding), plus independence of the
+deterministic adjoint (tensor-core gridding in colour launches, the kooshball
+centre's bins split into segments whose partial sums are added in order), plus
+independence of the
 result from the coil count (the tensor-core kernel's block shape depends on
 it). This covers the kooshball centre's bins split into several work items,
 the work-item order in 4x4x4-bin tiles and sample indices near 2^24.
@@ -69,7 +71,7 @@ def test_kooshball_fullsize_forward(koosh):
     assert e < TOL
 
 
-@pytest.mark.parametrize("deterministic", [False, True], ids=["tensor-core", "register-tile"])
+@pytest.mark.parametrize("deterministic", [False, True], ids=["atomic", "deterministic"])
 def test_kooshball_fullsize_adjoint(koosh, deterministic):
     F, R = koosh["F"], koosh["R"]
     dcf = koosh["dcf"]

@@ -1,5 +1,8 @@
-"""GPU parity of the 3D register-tile gridding (deterministic mode, batches of
-8 coils and more) against the oracle: regular and anisotropic grids (partial block regions at
+"""GPU parity of deterministic 3D gridding against the oracle: the tensor-core
+kernel in colour launches for widths 2..5 (heavy bins split into segments
+whose partial sums a reduction adds in order), the register-tile kernel for
+wider kernels and when the tensor-core path is switched off (DMR_NO_TC=1, in
+a child process): regular and anisotropic grids (partial block regions at
 the grid edge), several widths, coil counts that leave part of a 32-coil
 block empty, frames, a trajectory dense enough to split the central regions
 over several blocks, and bitwise reproducibility.
@@ -142,3 +145,42 @@ def test_regtile_batch_slices_agree(F):
     full = F.apply_nufft_adj(y, plan)
     part = F.apply_nufft_adj(y[8:24].contiguous(), plan)
     assert torch.equal(full[8:24], part)
+
+
+_RT_SCRIPT = r"""
+import numpy as np, torch
+import deepmr_b200.fft as F
+from deepmr_b200 import synth
+from oracle import nufft_ref as R
+F.set_deterministic_gridding(True)
+worst = 0.0
+for n, nc, w, os, seed in [(24, 16, 4, 1.25, 0), (20, 32, 3, 1.5, 1), (24, 12, 5, 1.25, 2)]:
+    coord = synth.kooshball_3d(2000, 48, n)
+    c = torch.as_tensor(coord)
+    y = synth.complex_gaussian((nc,) + tuple(c.shape[:-1]), seed=seed)
+    plan = F.plan_nufft(c, n, w, os, device="cuda")
+    a = F.apply_nufft_adj(y.cuda(), plan)
+    b = F.apply_nufft_adj(y.cuda(), plan)
+    assert torch.equal(a, b)
+    ref = R.apply_nufft_adj(y[:2], R.plan_nufft(c, n, w, os))
+    d = np.asarray(a[:2].cpu(), np.complex128) - np.asarray(ref, np.complex128)
+    worst = max(worst, float(np.linalg.norm(d) / np.linalg.norm(np.asarray(ref, np.complex128))))
+print("REL", worst)
+"""
+
+
+def test_register_tile_path_when_tensor_cores_off():
+    """The register-tile kernel (the deterministic path without the tensor-core
+    kernel) in a process started with DMR_NO_TC=1: oracle parity on dense
+    kooshballs (split regions) and bitwise reproducibility."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, DMR_NO_TC="1", PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    out = subprocess.run([sys.executable, "-c", _RT_SCRIPT], env=env, cwd=root, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    worst = float(out.stdout.split("REL")[-1])
+    assert worst < TOL
