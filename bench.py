@@ -566,7 +566,9 @@ def run_serving(dev, nreq=64, seed=0, max_active=4):
     {128, 192, 256, 320}^2, coils over {8, 16, 32}, radial or spiral): all
     requests at once (burst), then Poisson arrivals at 80% of the plain path's
     burst throughput. Both paths run every request set once untimed first
-    (plans, caching allocator, graphs). Latency = arrival to result on the host."""
+    (plans, caching allocator, graphs). Requests carry their k-space in pinned
+    host memory; latency = arrival to the result in host memory (upload,
+    AHy, CG and download included)."""
     from deepmr_b200 import recon
 
     burst = recon.synthetic_requests(nreq, rate_hz=1e6, seed=seed)

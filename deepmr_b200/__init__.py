@@ -2,7 +2,10 @@
 
 ``deepmr_b200.fft`` mirrors ``deepmr.fft``'s NUFFT API (plan_nufft, nufft,
 nufft_adj, apply_*, Toeplitz self-adjoint) on hand-written CUDA kernels behind
-the C ABI declared in ``include/deepmr_b200.h``.
+the C ABI declared in ``include/deepmr_b200.h``. Its callers in the reference
+are mirrored beside it: ``linops`` (NUFFT / SENSE operators, ``EncodingOp``),
+``optim`` (``cg_solve``), ``calib`` (``find_acs``, ``espirit_cal``) and
+``recon`` (device CG-SENSE and the serving loop).
 """
 
 from . import fft  # noqa: F401

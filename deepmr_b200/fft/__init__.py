@@ -64,9 +64,12 @@ __all__ = [
 def set_deterministic_gridding(flag=True):
     """Select the gridding kernel used by the adjoint NUFFT.
 
-    True: each grid tile is summed by one warp in a fixed sample order —
-    bitwise reproducible. False (default): shared-memory tiles flushed with
-    global atomics (summation order may vary between runs).
+    True: bitwise reproducible — 3D plans grid on the tensor cores in colour
+    launches (no two bins of a launch share a grid point; bins of more than
+    2048 samples are split into segments whose partial sums are added in a
+    fixed order), other plans with one owner per grid point or per tile.
+    False (default): grid-point additions with atomics (summation order may
+    vary between runs, results agree to float32 rounding).
     Returns the previous setting.
     """
     old = _nufft.DETERMINISTIC_GRIDDING

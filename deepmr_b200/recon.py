@@ -19,7 +19,12 @@ Here:
   that arrive while others run are admitted as slots and memory free up).
   Each request runs in a resident slot whose CG iteration is a captured CUDA
   graph (one launch per iteration). `run_sequential` is the plain per-call
-  path: one request at a time, to completion, with eager launches.
+  path: one request at a time, to completion, with eager launches. Requests
+  carry host k-space (pinned), uploaded on the slot's stream; a result is
+  copied back to pinned host memory before the request counts as done, so a
+  latency runs from arrival to the result on the host. A cancelled request, a
+  malformed one (coordinates, shapes) and one whose working set exceeds the
+  whole HBM budget produce an error status instead of a result (`Admission`).
 
 The CG reductions have a fixed order; with deterministic AHy gridding a
 request's result does not depend on what else runs beside it (bitwise), with
@@ -162,7 +167,7 @@ def cg_sense(kspace, coord, shape, maps, dcf=None, niter=20, lamda=0.0, tol=0.0,
 @dataclass
 class ReconRequest:
     rid: int
-    kspace: torch.Tensor  # (ncoils, nviews, nsamples) complex64
+    kspace: torch.Tensor  # (ncoils, nviews, nsamples) complex64, host (pinned) or device
     traj_key: str  # identifies the trajectory (plans are cached by it)
     coord: object  # (nviews, nsamples, ndim) grid units
     shape: tuple
@@ -172,6 +177,101 @@ class ReconRequest:
     niter: int = 20
     lamda: float = 0.0
     arrival: float = 0.0  # seconds after the start of the run
+    cancelled: bool = False
+
+    def cancel(self):
+        """Withdraw the request: not admitted if still waiting; if already
+        running, its result is dropped when it finishes (status "cancelled")."""
+        self.cancelled = True
+
+
+def _host_array(a):
+    if isinstance(a, torch.Tensor):
+        return a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
+def working_set_bytes(req):
+    """Device bytes one active request holds beside the resident caches: CG
+    vectors, AHy, the adjoint's oversampled grids and the Toeplitz buffers."""
+    ndim = len(req.shape)
+    isize = int(np.prod(req.shape))
+    ncoils = int(np.shape(req.kspace)[0]) if isinstance(req.kspace, np.ndarray) else int(req.kspace.shape[0])
+    G = int(np.prod([math.ceil(1.25 * s) for s in req.shape]))
+    K = int(np.prod([2 * s for s in req.shape]))
+    return 8 * (6 * isize + 2 * ncoils * G + ncoils * isize + ncoils * K) + (1 << 20) * ndim
+
+
+class Admission:
+    """Host-side admission of `ReconServer` (no device work).
+
+    FIFO over the requests that have arrived. The head request is rejected,
+    with a status message, when it was cancelled, when it is malformed
+    (non-finite or wrongly shaped coordinates; k-space, coil maps or density
+    weights whose shape does not match the trajectory and image), or when its
+    working set exceeds the whole HBM budget (it could never run). Otherwise it
+    is admitted while a slot is free and its working set fits beside the active
+    requests' (or nothing is active)."""
+
+    def __init__(self, budget, max_active, request_bytes, known_trajectories=()):
+        self.budget = int(budget)
+        self.max_active = int(max_active)
+        self.request_bytes = request_bytes
+        self.known = known_trajectories  # trajectory keys already checked (planned)
+
+    def validate(self, req):
+        """None if `req` can run, else the reason it cannot."""
+        if req.cancelled:
+            return "cancelled"
+        shape = tuple(int(n) for n in req.shape)
+        ndim = len(shape)
+        if ndim not in (1, 2, 3) or min(shape) < 1:
+            return f"malformed request: image shape {shape}"
+        if req.niter < 0:
+            return f"malformed request: niter {req.niter}"
+        if req.traj_key in self.known:
+            kshape = None
+        else:
+            coord = _host_array(req.coord)
+            if coord.ndim < 2 or coord.shape[-1] != ndim:
+                return f"malformed coordinates: shape {tuple(coord.shape)} for a {ndim}D image"
+            if not np.issubdtype(coord.dtype, np.number) or not np.isfinite(coord).all():
+                return "malformed coordinates: non-finite values"
+            kshape = tuple(coord.shape[:-1])
+        ksp_shape = tuple(torch.as_tensor(req.kspace).shape) if not isinstance(req.kspace, np.ndarray) \
+            else req.kspace.shape
+        if len(ksp_shape) < 2:
+            return f"malformed k-space: shape {ksp_shape}"
+        if kshape is not None and tuple(ksp_shape[1:]) != kshape:
+            return f"malformed k-space: shape {ksp_shape} for trajectory {kshape}"
+        maps_shape = tuple(np.shape(req.maps)) if not isinstance(req.maps, torch.Tensor) else tuple(req.maps.shape)
+        if maps_shape != (ksp_shape[0],) + shape:
+            return f"malformed coil maps: shape {maps_shape} for {ksp_shape[0]} coils and image {shape}"
+        if req.dcf is not None and kshape is not None and tuple(np.shape(req.dcf)) != kshape:
+            return f"malformed density weights: shape {tuple(np.shape(req.dcf))} for trajectory {kshape}"
+        nb = self.request_bytes(req)
+        if nb > self.budget:
+            return f"working set {nb} B exceeds the HBM budget {self.budget} B"
+        return None
+
+    def take(self, pending, now, realtime, nactive, used):
+        """Next decision for the head of `pending` (sorted by arrival), which it
+        pops: ("reject", req, reason) or ("admit", req, nbytes); None while the
+        head has not arrived, no slot is free or its working set does not fit."""
+        if not pending or (realtime and pending[0].arrival > now):
+            return None
+        req = pending[0]
+        reason = self.validate(req)
+        if reason is not None:
+            pending.pop(0)
+            return ("reject", req, reason)
+        if nactive >= self.max_active:
+            return None
+        nb = self.request_bytes(req)
+        if nactive and used + nb > self.budget:
+            return None
+        pending.pop(0)
+        return ("admit", req, nb)
 
 
 class _Slot:
@@ -224,10 +324,12 @@ class _Active:
 
 @dataclass
 class ServeStats:
-    latency: dict = field(default_factory=dict)  # rid -> seconds (arrival to result)
-    results: dict = field(default_factory=dict)  # rid -> image tensor
+    latency: dict = field(default_factory=dict)  # rid -> seconds (arrival to result on the host)
+    results: dict = field(default_factory=dict)  # rid -> image tensor (host)
+    errors: dict = field(default_factory=dict)  # rid -> why the request produced no result
     wall: float = 0.0
     peak_active: int = 0
+    peak_bytes: int = 0  # largest sum of active working sets
 
     def summary(self):
         lat = np.asarray(sorted(self.latency.values()))
@@ -236,7 +338,7 @@ class ServeStats:
         return {"requests": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "throughput_rps": float(lat.size / self.wall) if self.wall > 0 else None,
-                "wall_s": self.wall, "peak_active": self.peak_active}
+                "wall_s": self.wall, "peak_active": self.peak_active, "errors": len(self.errors)}
 
 
 class ReconServer:
@@ -282,13 +384,8 @@ class ReconServer:
         return self.normals[key]
 
     def request_bytes(self, req):
-        """Working set of one active request: CG vectors, AHy and the adjoint's grid workspace."""
-        ndim = len(req.shape)
-        isize = int(np.prod(req.shape))
-        ncoils = int(torch.as_tensor(req.kspace).shape[0])
-        G = int(np.prod([math.ceil(1.25 * s) for s in req.shape]))
-        K = int(np.prod([2 * s for s in req.shape]))
-        return 8 * (6 * isize + 2 * ncoils * G + ncoils * isize + ncoils * K) + (1 << 20) * ndim
+        """Working set of one active request (`working_set_bytes`)."""
+        return working_set_bytes(req)
 
     def prepare(self, requests):
         """Build the resident plans, Toeplitz kernels, coil maps (and cuFFT
@@ -311,14 +408,16 @@ class ReconServer:
         free = self.slots.setdefault(self._key(req), [])
         return free.pop() if free else _Slot(self._normal(req), self.dev, self.use_graphs)
 
-    def _start(self, req, now):
+    def _start(self, req, nbytes, now):
+        # plans and maps first: a request they reject takes no slot
+        plan, gram, dcf = self._plan(req)
+        normal = self._normal(req)
         slot = self._take_slot(req)
         with torch.cuda.stream(slot.stream):
-            plan, gram, dcf = self._plan(req)
-            normal = self._normal(req)
+            # k-space upload (asynchronous from pinned host memory) on the slot's stream
             y = torch.as_tensor(req.kspace).to(self.dev, torch.complex64, non_blocking=True)
             slot.start(sense_adjoint(y, plan, normal.maps, dcf, self.deterministic))
-        return _Active(req, slot, self.request_bytes(req), started=now)
+        return _Active(req, slot, nbytes, started=now)
 
     def run(self, requests, realtime=True):
         """Serve `requests` (their `arrival` times are honoured when realtime).
@@ -331,31 +430,47 @@ class ReconServer:
         stats = ServeStats()
         pending = sorted(requests, key=lambda r: r.arrival)
         active, used = [], 0
+        adm = Admission(self.budget, self.max_active, self.request_bytes, self.plans)
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
-            # admission: arrived, a free slot, and room in the HBM budget (FIFO)
-            while pending and (not realtime or pending[0].arrival <= now) and len(active) < self.max_active:
-                nb = self.request_bytes(pending[0])
-                if active and used + nb > self.budget:
+            # admission (FIFO): arrived, a free slot, room in the HBM budget;
+            # cancelled, malformed and over-budget requests get an error status
+            while True:
+                d = adm.take(pending, now, realtime, len(active), used)
+                if d is None:
                     break
-                req = pending.pop(0)
-                a = self._start(req, now)
+                kind, req, info = d
+                if kind == "reject":
+                    stats.errors[req.rid] = info
+                    continue
+                try:
+                    a = self._start(req, info, now)
+                except _lib.DmrError as e:
+                    stats.errors[req.rid] = str(e)
+                    continue
                 for _ in range(req.niter):
                     a.slot.step()
                 with torch.cuda.stream(a.slot.stream):
-                    a.result = a.slot.cg.x.clone()  # the slot is reused: the result leaves it
+                    # the result leaves the slot (reused) for pinned host memory
+                    x = a.slot.cg.x
+                    a.result = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+                    a.result.copy_(x, non_blocking=True)
                 a.done_event = torch.cuda.Event()
                 a.done_event.record(a.slot.stream)
                 active.append(a)
-                used += nb
+                used += info
+                stats.peak_bytes = max(stats.peak_bytes, used)
             stats.peak_active = max(stats.peak_active, len(active))
             # retire finished requests
             still = []
             for a in active:
                 if a.done_event.query():
-                    stats.latency[a.req.rid] = time.perf_counter() - t0 - a.req.arrival
-                    stats.results[a.req.rid] = a.result
+                    if a.req.cancelled:
+                        stats.errors[a.req.rid] = "cancelled"
+                    else:
+                        stats.latency[a.req.rid] = time.perf_counter() - t0 - a.req.arrival
+                        stats.results[a.req.rid] = a.result
                     self.slots[self._key(a.req)].append(a.slot)
                     used -= a.nbytes
                 else:
@@ -374,21 +489,30 @@ class ReconServer:
     def run_sequential(self, requests, realtime=True):
         """Plain per-call path: one request at a time, to completion, on one stream."""
         stats = ServeStats()
+        adm = Admission(self.budget, 1, self.request_bytes, self.plans)
         t0 = time.perf_counter()
         for req in sorted(requests, key=lambda r: r.arrival):
             now = time.perf_counter() - t0
             if realtime and req.arrival > now:
                 time.sleep(req.arrival - now)
-            plan, gram, dcf = self._plan(req)
-            normal = self._normal(req)
+            reason = adm.validate(req)
+            if reason is not None:
+                stats.errors[req.rid] = reason
+                continue
+            try:
+                plan, gram, dcf = self._plan(req)
+                normal = self._normal(req)
+            except _lib.DmrError as e:
+                stats.errors[req.rid] = str(e)
+                continue
             y = torch.as_tensor(req.kspace).to(self.dev, torch.complex64)
             cg = CGState(sense_adjoint(y, plan, normal.maps, dcf, self.deterministic), normal)
             cg.init()
             for _ in range(req.niter):
                 cg.step()
-            torch.cuda.synchronize(self.dev)
+            x = cg.x.cpu()
             stats.latency[req.rid] = time.perf_counter() - t0 - req.arrival
-            stats.results[req.rid] = cg.x
+            stats.results[req.rid] = x
         stats.wall = time.perf_counter() - t0
         stats.peak_active = 1
         return stats
@@ -434,5 +558,6 @@ def synthetic_requests(n, rate_hz, seed=0, sizes=(128, 192, 256, 320), coils=(8,
         plan = nf.plan_nufft(torch.as_tensor(coord), N, 4, 1.25, "cuda")
         y = nf.apply_nufft(x.cuda(), plan)
         y = y + 1e-2 * synth.complex_gaussian(tuple(y.shape), seed=1000 + i, device="cuda")
-        reqs.append(ReconRequest(i, y, tkey, coord, (N, N), mkey, maps, dcf, niter, 0.0, t))
+        # requests arrive with their k-space in pinned host memory
+        reqs.append(ReconRequest(i, y.cpu().pin_memory(), tkey, coord, (N, N), mkey, maps, dcf, niter, 0.0, t))
     return reqs

@@ -20,15 +20,19 @@ def golden_cases(prefix=None, kind="nufft"):
     lowrank = [n for n in names if n.startswith("lowrank")]
     sparse = [n for n in names if n.startswith("sparse")]
     cgsense = [n for n in names if n.startswith("cgsense")]
+    calib = [n for n in names if n.startswith("calib")]
     if kind == "cgsense":
         return cgsense
+    if kind == "calib":
+        return calib
     if kind == "toeplitz":
         return toep
     if kind == "lowrank":
         return lowrank
     if kind == "sparse":
         return sparse
-    return [n for n in names if n not in toep and n not in lowrank and n not in sparse and n not in cgsense]
+    other = set(toep) | set(lowrank) | set(sparse) | set(cgsense) | set(calib)
+    return [n for n in names if n not in other]
 
 
 @pytest.fixture

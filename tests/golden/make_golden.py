@@ -7,6 +7,8 @@ the ``DEEPMR_REFERENCE`` environment variable (the project root, containing
     DEEPMR_REFERENCE=/path/to/deep-mr python tests/golden/make_golden.py   # every case
     python tests/golden/make_golden.py lowrank    # only the low-rank cases
     python tests/golden/make_golden.py sparse     # only the sparse FFT cases
+    python tests/golden/make_golden.py cgsense    # only the CG-SENSE case
+    python tests/golden/make_golden.py calib      # only the calibration cases
 
 The reference's top-level package import needs optional I/O dependencies that
 are absent, so the script registers stub parent packages whose ``__path__``
@@ -122,6 +124,86 @@ def cgsense_case(name="cgsense2d", N=128, ncoils=8, nspokes=96, nsamples=256, ni
 
 def _np(x):
     return x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)
+
+
+def import_reference_calib():
+    """The reference's calibration callers of the NUFFT (deepmr.recon.calib.acs,
+    .espirit) through stub parents; deepmr._signal gets the functions its
+    package __init__ would re-export (resize, resample, rss)."""
+    import_reference()
+    for name, sub in [("deepmr.recon", "/recon"), ("deepmr.recon.calib", "/recon/calib")]:
+        mod = types.ModuleType(name)
+        mod.__path__ = [REF_SRC + sub]
+        sys.modules[name] = mod
+    import deepmr._signal.subspace  # noqa: F401
+
+    resize_mod, subspace_mod = sys.modules["deepmr._signal.resize"], sys.modules["deepmr._signal.subspace"]
+    sig = sys.modules["deepmr._signal"]
+    sig.resize, sig.resample, sig.rss = resize_mod.resize, resize_mod.resample, subspace_mod.rss
+    import deepmr.recon.calib.acs as acs  # noqa: E402
+    import deepmr.recon.calib.espirit as espirit  # noqa: E402
+
+    return acs, espirit
+
+
+def calib_cases(seed=0):
+    """Calibration callers of the reference on NUFFT data.
+
+    calib2d: 2D golden-angle radial (128 spokes x 192 samples, 96^2 image,
+    8 coils, ramp density weights), k-space = the reference's forward NUFFT of
+    coil maps x phantom plus noise, in the 2D non-Cartesian layout (nslices=1,
+    ncoils, ncontrasts=1, nviews, nsamples): find_acs (_find_noncart_acs,
+    src/deepmr/recon/calib/acs.py:117-152, calibration grid 64^2) and
+    espirit_cal (src/deepmr/recon/calib/espirit.py:14-223, k=6, r=24, t=0.02,
+    c=0) maps and calibration data.
+    calib3d: 3D golden-means kooshball (600 spokes x 48 samples, 24^3 image,
+    4 coils): find_acs with a 16^3 calibration grid."""
+    N, F = import_reference()
+    acs, espirit = import_reference_calib()
+    n, nc = 96, 8
+    coord = torch.as_tensor(synth.radial_2d(128, 192, n))
+    dcf = torch.as_tensor(synth.ramp_dcf(coord.numpy()))
+    maps = torch.as_tensor(synth.coil_maps(nc, (n, n), seed=seed + 3))
+    img = torch.as_tensor(synth.ellipse_phantom(n, seed=seed + 4)).to(torch.complex64) * maps
+    y = F.nufft(img, coord, shape=n)  # (ncoils, nviews, nsamples)
+    g = torch.Generator().manual_seed(seed + 9)
+    y = (y + 1e-3 * torch.complex(torch.randn(y.shape, generator=g), torch.randn(y.shape, generator=g))).to(
+        torch.complex64)
+    data = y[None, :, None]  # (nslices, ncoils, ncontrasts, nviews, nsamples)
+    cal = acs.find_acs(data, [64, 64], coord, dcf)
+    emaps, ecal = espirit.espirit_cal(data, coord=coord, dcf=dcf, shape=n)
+    np.savez_compressed(os.path.join(HERE, "calib2d.npz"), coord=_np(coord), dcf=_np(dcf), kspace=_np(data),
+                        shape=np.int32(n), acs=_np(cal), maps=_np(emaps), cal=_np(ecal))
+    print("wrote calib2d")
+
+    n3, nc3 = 24, 4
+    coord3 = torch.as_tensor(synth.kooshball_3d(600, 48, n3))
+    img3 = torch.as_tensor(synth.complex_gaussian((nc3, n3, n3, n3), seed=seed + 11))
+    y3 = F.nufft(img3, coord3, shape=n3)[:, None]  # (ncoils, ncontrasts, nviews, nsamples)
+    cal3 = acs.find_acs(y3, [16, 16, 16], coord3, None)
+    np.savez_compressed(os.path.join(HERE, "calib3d.npz"), coord=_np(coord3), kspace=_np(y3),
+                        shape=np.int32(n3), acs=_np(cal3))
+    print("wrote calib3d")
+
+    # Cartesian find_acs (acs.py:54-114) on undersampled 2D multi-slice data
+    # (fully sampled 10 x 8 centre, every other line outside), and the signal
+    # helpers espirit_cal uses (resample up and down, rss, fermi)
+    g = torch.Generator().manual_seed(seed + 13)
+    cart = torch.complex(torch.randn(2, 4, 2, 32, 24, generator=g), torch.randn(2, 4, 2, 32, 24, generator=g))
+    mask = torch.zeros(32, 24, dtype=torch.bool)
+    mask[::2, :] = True
+    mask[11:21, 8:16] = True
+    cart = cart * mask
+    cal_cart = acs.find_acs(cart)
+    sig = sys.modules["deepmr._signal"]
+    filt_mod = sys.modules["deepmr._signal.filter"]
+    x = torch.complex(torch.randn(3, 16, 20, generator=g), torch.randn(3, 16, 20, generator=g))
+    xr = torch.randn(3, 16, 20, generator=g)
+    np.savez_compressed(os.path.join(HERE, "calib_cart.npz"), kspace=_np(cart), acs=_np(cal_cart),
+                        x=_np(x), x_up=_np(sig.resample(x, [24, 24])), x_down=_np(sig.resample(x, [12, 14])),
+                        xr=_np(xr), xr_up=_np(sig.resample(xr, [24, 24])), x_rss=_np(sig.rss(x, axis=0)),
+                        fermi=_np(filt_mod.fermi(2, 24, 10)))
+    print("wrote calib_cart")
 
 
 def nufft_case(N, F, name, coord, shape, batch_shape, width, oversamp, weight=None,
@@ -285,6 +367,9 @@ def main():
     if sys.argv[1:] == ["sparse"]:
         sparse_cases()
         return
+    if sys.argv[1:] == ["calib"]:
+        calib_cases()
+        return
 
     # 2D golden-angle radial, width 3 / oversampling 2 (the 2D benchmark's kernel)
     c = synth.radial_2d(16, 32, 32)
@@ -348,6 +433,7 @@ def main():
     lowrank_cases(N)
     sparse_cases()
     cgsense_case()
+    calib_cases()
 
 
 if __name__ == "__main__":

@@ -160,10 +160,52 @@ def test_serving_admission_respects_budget():
     from deepmr_b200 import recon
 
     reqs = _requests()
-    server = recon.ReconServer(device="cuda", max_active=6,
-                               hbm_budget=min(recon.ReconServer().request_bytes(r) for r in reqs))
+    budget = max(recon.working_set_bytes(r) for r in reqs)
+    server = recon.ReconServer(device="cuda", max_active=6, hbm_budget=budget)
     server.prepare(reqs)
     stats = server.run(reqs, realtime=False)
-    assert stats.peak_active == 1 and len(stats.results) == len(reqs)
+    assert 0 < stats.peak_bytes <= budget and len(stats.results) == len(reqs) and not stats.errors
     s = stats.summary()
     assert s["requests"] == len(reqs) and s["p99_ms"] >= s["p50_ms"] > 0
+    # results come back on the host
+    assert all(x.device.type == "cpu" for x in stats.results.values())
+
+
+def test_serving_error_statuses_and_the_rest_served():
+    """Cancelled (before and while running), malformed and over-budget requests
+    produce an error status; the others' results equal the plain path's."""
+    import dataclasses
+
+    import numpy as np
+
+    from deepmr_b200 import recon
+
+    reqs = _requests()
+    budget = max(recon.working_set_bytes(r) for r in reqs)
+    bad_coord = np.array(reqs[0].coord, dtype=np.float32, copy=True)
+    bad_coord[0, 0, 0] = np.nan
+    extra = [
+        dataclasses.replace(reqs[1], rid=100, cancelled=True),
+        dataclasses.replace(reqs[0], rid=101, traj_key="nan-coords", coord=bad_coord),
+        dataclasses.replace(reqs[2], rid=102, shape=(512, 512), maps_key="big",
+                            maps=np.zeros((reqs[2].kspace.shape[0], 512, 512), np.complex64)),
+        dataclasses.replace(reqs[3], rid=103),
+    ]
+
+    class CancelWhileRunning(recon.ReconServer):
+        def _start(self, req, nbytes, now):
+            a = super()._start(req, nbytes, now)
+            if req.rid == 103:
+                req.cancel()
+            return a
+
+    server = CancelWhileRunning(device="cuda", max_active=6, hbm_budget=budget, deterministic=True)
+    server.prepare(reqs)
+    stats = server.run(reqs + extra, realtime=False)
+    assert stats.errors[100] == "cancelled" and stats.errors[103] == "cancelled"
+    assert stats.errors[101].startswith("malformed coordinates")
+    assert "exceeds the HBM budget" in stats.errors[102]
+    assert set(stats.results) == {r.rid for r in reqs}
+    ref = server.run_sequential(reqs, realtime=False)
+    for r in reqs:
+        assert torch.equal(stats.results[r.rid], ref.results[r.rid]), r.rid
