@@ -1,0 +1,680 @@
+// 3D FFT passes of the NUFFT pipelines, fused with the zero-padding /
+// cropping and the apodisation, and pruned to the lines that hold data.
+//
+// The forward NUFFT (src/deepmr/fft/nufft.py:450-528) apodises the image,
+// zero-pads it to the oversampled grid (src/deepmr/_signal/resize.py:11-102),
+// and takes a centred FFT (src/deepmr/fft/fft.py:9-87); the adjoint
+// (nufft.py:531-606) takes a centred inverse FFT (norm "backward", 1/G), crops
+// and apodises. The grid lives in FFT order (centred index c at
+// (c - G//2) mod G), so image index i of an axis sits at grid index
+// (i - N//2) mod G, and only N of the G positions of an axis hold image data.
+// A 3D transform is three passes of 1D transforms, and each pass touches only
+// the lines that matter:
+//   forward: x rows of the N1*N2 image rows (reading the image, apodising and
+//   padding on the fly), y columns of the N2 planes with data (reading only
+//   the N1 valid y), z columns everywhere (reading only the N2 valid z);
+//   adjoint: z columns everywhere (writing only the N2 kept z), y columns of
+//   the N2 kept planes (writing only the N1 kept y), x rows of the N1*N2 kept
+//   rows (writing the cropped, scaled, apodised image directly).
+// With G = 1.25 N that is 15.5 GB of DRAM traffic per 240^3 x 32 transform
+// against 26.6 GB for a full-grid pad kernel plus three full passes.
+//
+// Each block transforms 16 lines at once in one shared-memory buffer
+// ([position][line], line pitch 17 so that 8-byte accesses of a half-warp hit
+// distinct banks): a Stockham autosort FFT (Govindaraju et al., "High performance discrete
+// Fourier transforms on graphics processors", SC 2008) with radix-4, 2, 3 and
+// 5 stages, twiddles from a per-length table computed in double precision on
+// the host.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "plan.cuh"
+
+namespace dmr {
+
+namespace {
+
+constexpr int kFftLines = 16;  // lines per block
+constexpr int kFftLP = 17;     // shared-memory pitch of a position (lines + 1)
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// R-point DFT of v in place, V[m] = sum_q v[q] w^(q m), w = exp(-+2 pi i / R),
+// for R = 2, 4 (no multiplications), 3 and 5 (roots of unity from the table
+// of the transform length L)
+template <int R, int L>
+__device__ __forceinline__ void small_dft(float2 *v, const float2 *tw, bool inv)
+{
+    if constexpr (R == 2) {
+        const float2 a = v[0], b = v[1];
+        v[0] = make_float2(a.x + b.x, a.y + b.y);
+        v[1] = make_float2(a.x - b.x, a.y - b.y);
+    } else if constexpr (R == 4) {
+        const float2 s02 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
+        const float2 d02 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
+        const float2 s13 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
+        const float2 d13 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+        // w d13 with w = -i (forward) or +i (inverse)
+        const float2 jd = inv ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
+        v[0] = make_float2(s02.x + s13.x, s02.y + s13.y);
+        v[1] = make_float2(d02.x + jd.x, d02.y + jd.y);
+        v[2] = make_float2(s02.x - s13.x, s02.y - s13.y);
+        v[3] = make_float2(d02.x - jd.x, d02.y - jd.y);
+    } else if constexpr (R == 3) {
+        // w^2 = conj(w): V1,2 = v0 + Re(w) (v1 + v2) +- i Im(w) (v1 - v2)
+        float2 w = tw[L / 3];
+        if (inv) w.y = -w.y;
+        const float2 a = make_float2(v[1].x + v[2].x, v[1].y + v[2].y);
+        const float2 b = make_float2(v[1].x - v[2].x, v[1].y - v[2].y);
+        const float2 m = make_float2(v[0].x + w.x * a.x, v[0].y + w.x * a.y);
+        const float2 ib = make_float2(-w.y * b.y, w.y * b.x);
+        v[0] = make_float2(v[0].x + a.x, v[0].y + a.y);
+        v[1] = make_float2(m.x + ib.x, m.y + ib.y);
+        v[2] = make_float2(m.x - ib.x, m.y - ib.y);
+    } else {
+        static_assert(R == 5, "radix");
+        // w^4 = conj(w), w^3 = conj(w^2); a1 = v1 + v4, b1 = v1 - v4,
+        // a2 = v2 + v3, b2 = v2 - v3:
+        // V1,4 = v0 + Re(w) a1 + Re(w2) a2 +- i (Im(w) b1 + Im(w2) b2)
+        // V2,3 = v0 + Re(w2) a1 + Re(w) a2 +- i (Im(w2) b1 - Im(w) b2)
+        float2 w1 = tw[L / 5], w2 = tw[2 * (L / 5)];
+        if (inv) {
+            w1.y = -w1.y;
+            w2.y = -w2.y;
+        }
+        const float2 a1 = make_float2(v[1].x + v[4].x, v[1].y + v[4].y);
+        const float2 b1 = make_float2(v[1].x - v[4].x, v[1].y - v[4].y);
+        const float2 a2 = make_float2(v[2].x + v[3].x, v[2].y + v[3].y);
+        const float2 b2 = make_float2(v[2].x - v[3].x, v[2].y - v[3].y);
+        const float2 m1 = make_float2(v[0].x + w1.x * a1.x + w2.x * a2.x, v[0].y + w1.x * a1.y + w2.x * a2.y);
+        const float2 m2 = make_float2(v[0].x + w2.x * a1.x + w1.x * a2.x, v[0].y + w2.x * a1.y + w1.x * a2.y);
+        const float2 s1 = make_float2(w1.y * b1.x + w2.y * b2.x, w1.y * b1.y + w2.y * b2.y);
+        const float2 s2 = make_float2(w2.y * b1.x - w1.y * b2.x, w2.y * b1.y - w1.y * b2.y);
+        v[0] = make_float2(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
+        v[1] = make_float2(m1.x - s1.y, m1.y + s1.x);
+        v[4] = make_float2(m1.x + s1.y, m1.y - s1.x);
+        v[2] = make_float2(m2.x - s2.y, m2.y + s2.x);
+        v[3] = make_float2(m2.x + s2.y, m2.y - s2.x);
+    }
+}
+
+template <int M>
+struct Split {
+    static constexpr int A = M % 4 == 0 ? 4 : (M % 2 == 0 ? 2 : (M % 3 == 0 ? 3 : 5));
+    static constexpr int B = M / A;
+};
+
+// M-point DFT of registers v (M divides L), natural order in and out: radix
+// 2 / 3 / 4 / 5 directly, else M = A B in registers (index n = B n1 + n2):
+// A-point DFTs over n1, twiddles w_M^(n2 k1), B-point DFTs over n2, output
+// k1 + A k2. Every index is a compile-time constant once unrolled.
+template <int M, int L>
+__device__ __forceinline__ void reg_dft(float2 *v, const float2 *tw, bool inv)
+{
+    if constexpr (M == 2 || M == 3 || M == 4 || M == 5) {
+        small_dft<M, L>(v, tw, inv);
+    } else {
+        constexpr int A = Split<M>::A, B = Split<M>::B;
+        float2 y[M];
+#pragma unroll
+        for (int n2 = 0; n2 < B; n2++) {
+            float2 a[A];
+#pragma unroll
+            for (int n1 = 0; n1 < A; n1++) a[n1] = v[B * n1 + n2];
+            reg_dft<A, L>(a, tw, inv);
+#pragma unroll
+            for (int k1 = 0; k1 < A; k1++) {
+                if ((n2 * k1) % M != 0) {
+                    float2 w = tw[((n2 * k1) % M) * (L / M)];
+                    if (inv) w.y = -w.y;
+                    a[k1] = cmulf(a[k1], w);
+                }
+                y[n2 * A + k1] = a[k1];
+            }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < A; k1++) {
+            float2 b[B];
+#pragma unroll
+            for (int n2 = 0; n2 < B; n2++) b[n2] = y[n2 * A + k1];
+            reg_dft<B, L>(b, tw, inv);
+#pragma unroll
+            for (int k2 = 0; k2 < B; k2++) v[k1 + A * k2] = b[k2];
+        }
+    }
+}
+
+// A transform length L = L1 L2 (both at most 24, products of 2, 3, 4, 5).
+template <int L_, int L1_, int L2_>
+struct Len {
+    static constexpr int L = L_, L1 = L1_, L2 = L2_;
+    // one thread per (line, column) of step A and per (line, row) of step B
+    static constexpr int T = kFftLines * (L1 > L2 ? L1 : L2);
+    static_assert(L1 * L2 == L, "factors");
+};
+
+// Step A of the four-step transform of the block's 16 lines in buf
+// ([position][line]): line c, column n2 takes positions L2 n1 + n2, an
+// L1-point DFT, twiddles w_L^(n2 k1), back to positions L2 k1 + n2 (the
+// positions it read: no barrier needed between its reads and writes).
+template <class F>
+__device__ __forceinline__ void step_a(float2 *buf, const float2 *tw, bool inv)
+{
+    constexpr int L = F::L, L1 = F::L1, L2 = F::L2;
+    const int w = threadIdx.x;
+    if (w < kFftLines * L2) {
+        const int c = w & (kFftLines - 1), n2 = w >> 4;
+        float2 a[L1];
+#pragma unroll
+        for (int n1 = 0; n1 < L1; n1++) a[n1] = buf[(L2 * n1 + n2) * kFftLP + c];
+        reg_dft<L1, L>(a, tw, inv);
+#pragma unroll
+        for (int k1 = 1; k1 < L1; k1++) {
+            float2 t = tw[(n2 * k1) % L];
+            if (inv) t.y = -t.y;
+            a[k1] = cmulf(a[k1], t);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < L1; k1++) buf[(L2 * k1 + n2) * kFftLP + c] = a[k1];
+    }
+}
+
+// Step B for line c, row k1: positions L2 k1 + n2 (n2 < L2), an L2-point DFT;
+// b[k2] is the transform at position k1 + L1 k2.
+template <class F>
+__device__ __forceinline__ void step_b(const float2 *buf, const float2 *tw, bool inv, int c, int k1, float2 *b)
+{
+    constexpr int L = F::L, L2 = F::L2;
+#pragma unroll
+    for (int n2 = 0; n2 < L2; n2++) b[n2] = buf[(L2 * k1 + n2) * kFftLP + c];
+    reg_dft<L2, L>(b, tw, inv);
+}
+
+// the lengths with a compiled transform (grid extents of common matrix sizes
+// at oversampling 1.25 and 2), as (L, L1, L2); other lengths use cuFFT
+#define DMR_FFT_LENGTHS(X)                                                                            \
+    X(32, 8, 4) X(40, 8, 5) X(48, 16, 3) X(64, 8, 8) X(80, 16, 5) X(96, 16, 6) X(120, 12, 10)           \
+    X(128, 16, 8) X(144, 12, 12) X(160, 16, 10) X(192, 16, 12) X(200, 20, 10) X(240, 16, 15)            \
+    X(256, 16, 16) X(288, 18, 16) X(320, 20, 16) X(384, 24, 16) X(400, 20, 20) X(480, 24, 20)
+
+bool has_len(int L)
+{
+    switch (L) {
+#define DMR_FFT_CASE(L, L1, L2) case L: return true;
+        DMR_FFT_LENGTHS(DMR_FFT_CASE)
+#undef DMR_FFT_CASE
+    default: return false;
+    }
+}
+
+struct FftGeom {
+    int N[3], G[3];       // image / grid extents (x, y, z)
+    int64_t nbf;          // batch * frames
+    int64_t gsize, isize; // points per grid / image
+    const float *apod[3]; // per-axis apodisation by image index (nullptr: 1)
+    float scale;
+};
+
+__host__ __device__ __forceinline__ int wrapi(int v, int n)
+{
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+// whether position l of a length-L line lies in the cyclic range [q0, q0 + n)
+__device__ __forceinline__ bool in_range(int l, int q0, int n, int L)
+{
+    int d = l - q0;
+    if (d < 0) d += L;
+    return d < n;
+}
+
+// asynchronous copy of `bytes` (4 or 8) into shared memory; when !valid the
+// destination is zero-filled and nothing is read (src must still be mapped)
+__device__ __forceinline__ void cp_async_fill(void *sdst, const void *src, int bytes, bool valid)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    const int n = valid ? bytes : 0;
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Per-line data of a row tile, computed once by the first 16 threads: the
+// image row offset, the grid row offset and the apodisation of the row's
+// (y, z) times the scale; rows past the end get offset -1.
+struct RowLine {
+    int64_t img, grid;
+    float s;
+};
+
+__device__ __forceinline__ void row_lines(const FftGeom &g, int64_t row0, int64_t nrows, RowLine *lines)
+{
+    const int c = threadIdx.x;
+    if (c >= kFftLines) return;
+    const int64_t row = row0 + c;
+    RowLine ln;
+    ln.img = -1;
+    ln.grid = -1;
+    ln.s = 0.0f;
+    if (row < nrows) {
+        const int N1 = g.N[1], N2 = g.N[2];
+        const int64_t plane = (int64_t)N2 * N1;
+        const int64_t bf = row / plane;
+        const int rr = (int)(row - bf * plane);
+        const int y = rr % N1, z = rr / N1;
+        const int qy = wrapi(y - N1 / 2, g.G[1]), qz = wrapi(z - N2 / 2, g.G[2]);
+        ln.img = bf * g.isize + (int64_t)rr * g.N[0];
+        ln.grid = bf * g.gsize + ((int64_t)qz * g.G[1] + qy) * g.G[0];
+        float s = g.scale;
+        if (g.apod[1]) s *= g.apod[1][y];
+        if (g.apod[2]) s *= g.apod[2][z];
+        ln.s = s;
+    }
+    lines[c] = ln;
+}
+
+// Row passes (x): tiles of 16 rows, double-buffered (the next tile's loads
+// are in flight while the current one is transformed); shared memory holds
+// two [L][17] tiles, the twiddle table and the x apodisation.
+//   forward (CROP false): image rows (real or complex) are placed at their
+//   FFT-order positions (zero elsewhere), apodised, transformed and written
+//   as full grid rows;
+//   adjoint (CROP true): grid rows are inverse-transformed and the kept x,
+//   scaled and apodised, written to the image.
+template <class F, bool CROP>
+__global__ void __launch_bounds__(F::T) fft_rows_kernel(FftGeom g, const float2 *__restrict__ tw,
+                                                        const void *__restrict__ src, int src_real,
+                                                        float2 *__restrict__ dst)
+{
+    constexpr int L = F::L, L1 = F::L1, L2 = F::L2, T = F::T;
+    extern __shared__ __align__(16) float2 fsm[];
+    float2 *bufs = fsm;                               // 2 x L * 17
+    float2 *tws = fsm + 2 * L * kFftLP;               // L
+    float *apx = reinterpret_cast<float *>(tws + L);  // L: x apodisation by image index
+    __shared__ RowLine lines[2][kFftLines];
+    for (int i = threadIdx.x; i < L; i += T) {
+        tws[i] = tw[i];
+        apx[i] = (g.apod[0] && i < g.N[0]) ? g.apod[0][i] : 1.0f;
+    }
+    const int N0 = g.N[0], h0 = N0 / 2;
+    const int64_t nrows = g.nbf * g.N[2] * g.N[1];
+    const int64_t ntiles = (nrows + kFftLines - 1) / kFftLines;
+    // loads of tile t into buffer `slot` (line data first, so a barrier)
+    auto prefetch = [&](int64_t t, int slot) {
+        row_lines(g, t * kFftLines, nrows, lines[slot]);
+        __syncthreads();
+        float2 *buf = bufs + slot * L * kFftLP;
+        for (int e = threadIdx.x; e < kFftLines * L; e += T) {
+            const int c = e / L, q = e - c * L;
+            const RowLine ln = lines[slot][c];
+            float2 *d = buf + q * kFftLP + c;
+            if (!CROP) {
+                int i = q + h0;
+                if (i >= L) i -= L;
+                const bool ok = ln.img >= 0 && i < N0;
+                if (src_real) {
+                    const float *sp = reinterpret_cast<const float *>(src) + (ok ? ln.img + i : 0);
+                    cp_async_fill(d, sp, 4, ok);
+                    cp_async_fill(reinterpret_cast<float *>(d) + 1, sp, 4, false);
+                } else {
+                    cp_async_fill(d, reinterpret_cast<const float2 *>(src) + (ok ? ln.img + i : 0), 8, ok);
+                }
+            } else {
+                const bool ok = ln.grid >= 0;
+                cp_async_fill(d, reinterpret_cast<const float2 *>(src) + (ok ? ln.grid + q : 0), 8, ok);
+            }
+        }
+        cp_async_commit();
+    };
+    int64_t t = blockIdx.x;
+    if (t < ntiles) prefetch(t, 0);
+    for (int it = 0; t < ntiles; t += gridDim.x, it++) {
+        const int cur = it & 1;
+        float2 *buf = bufs + cur * L * kFftLP;
+        if (t + gridDim.x < ntiles) prefetch(t + gridDim.x, cur ^ 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (!CROP) {
+            // apodisation: position q of line c holds image index (q + N0/2) mod L, or zero
+            for (int e = threadIdx.x; e < kFftLines * L; e += T) {
+                const int q = e >> 4, c = e & (kFftLines - 1);
+                int i = q + h0;
+                if (i >= L) i -= L;
+                const float sc = lines[cur][c].s * (i < N0 ? apx[i] : 0.0f);
+                float2 &v = buf[q * kFftLP + c];
+                v.x *= sc;
+                v.y *= sc;
+            }
+            __syncthreads();
+        }
+        step_a<F>(buf, tws, CROP);
+        __syncthreads();
+        // step B into registers, then (after every thread has read its
+        // inputs) back into the tile in transform order
+        const int w = threadIdx.x;
+        const int c = w & (kFftLines - 1), k1 = w >> 4;
+        float2 b[L2];
+        if (k1 < L1) step_b<F>(buf, tws, CROP, c, k1, b);
+        __syncthreads();
+        if (k1 < L1) {
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) buf[(k1 + L1 * k2) * kFftLP + c] = b[k2];
+        }
+        __syncthreads();
+        if (!CROP) {
+            for (int e = threadIdx.x; e < kFftLines * L; e += T) {
+                const int cc = e / L, l = e - cc * L;
+                const int64_t go = lines[cur][cc].grid;
+                if (go >= 0) dst[go + l] = buf[l * kFftLP + cc];
+            }
+        } else {
+            for (int e = threadIdx.x; e < kFftLines * N0; e += T) {
+                const int cc = e / N0, i = e - cc * N0;
+                const RowLine ln = lines[cur][cc];
+                if (ln.img < 0) continue;
+                int q = i - h0;
+                if (q < 0) q += L;
+                float2 v = buf[q * kFftLP + cc];
+                const float sc = ln.s * apx[i];
+                v.x *= sc;
+                v.y *= sc;
+                dst[ln.img + i] = v;
+            }
+        }
+        // the tile's buffer is loaded again two iterations on
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// Column pass along y or z, in place on the grid: tiles of 16 consecutive x
+// of one line set (batch*frame, outer index), the line running along the axis
+// with element stride S. Input positions outside [in_q0, in_q0 + in_n)
+// (cyclic) are zero and not read; outputs outside [out_q0, out_q0 + out_n)
+// are not written. Outer index k in [0, nouter) selects plane / row
+// (outer_q0 + k) mod outer_G with stride outer_stride. Double-buffered like
+// the row passes; step B writes straight to the grid (16 consecutive x per
+// half-warp).
+struct ColArgs {
+    int64_t S, outer_stride;
+    int nouter, outer_q0, outer_G;
+    int in_q0, in_n, out_q0, out_n;
+    int inv;
+};
+
+template <class F>
+__global__ void __launch_bounds__(F::T) fft_cols_kernel(FftGeom g, ColArgs a, const float2 *__restrict__ tw,
+                                                        float2 *grid)
+{
+    constexpr int L = F::L, L1 = F::L1, L2 = F::L2, T = F::T;
+    extern __shared__ __align__(16) float2 fsm[];
+    float2 *bufs = fsm, *tws = fsm + 2 * L * kFftLP;
+    for (int i = threadIdx.x; i < L; i += T) tws[i] = tw[i];
+    const int G0 = g.G[0];
+    const int ntx = (G0 + kFftLines - 1) / kFftLines;
+    const int64_t ntiles = g.nbf * a.nouter * ntx;
+    const bool inv = a.inv != 0;
+    // first x and base pointer of tile t
+    auto tile = [&](int64_t t, int &x0) -> float2 * {
+        const int tx = (int)(t % ntx);
+        const int64_t rest = t / ntx;
+        const int k = (int)(rest % a.nouter);
+        const int64_t bf = rest / a.nouter;
+        int qo = a.outer_q0 + k;
+        if (qo >= a.outer_G) qo -= a.outer_G;
+        x0 = tx * kFftLines;
+        return grid + bf * g.gsize + (int64_t)qo * a.outer_stride + x0;
+    };
+    auto prefetch = [&](int64_t t, int slot) {
+        int x0;
+        const float2 *base = tile(t, x0);
+        float2 *buf = bufs + slot * L * kFftLP;
+        for (int e = threadIdx.x; e < kFftLines * L; e += T) {
+            const int l = e >> 4, c = e & (kFftLines - 1);
+            const bool ok = x0 + c < G0 && in_range(l, a.in_q0, a.in_n, L);
+            cp_async_fill(buf + l * kFftLP + c, ok ? base + (int64_t)l * a.S + c : base, 8, ok);
+        }
+        cp_async_commit();
+    };
+    int64_t t = blockIdx.x;
+    if (t < ntiles) prefetch(t, 0);
+    for (int it = 0; t < ntiles; t += gridDim.x, it++) {
+        const int cur = it & 1;
+        float2 *buf = bufs + cur * L * kFftLP;
+        if (t + gridDim.x < ntiles) prefetch(t + gridDim.x, cur ^ 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        step_a<F>(buf, tws, inv);
+        __syncthreads();
+        const int w = threadIdx.x;
+        const int c = w & (kFftLines - 1), k1 = w >> 4;
+        int x0;
+        float2 *base = tile(t, x0);
+        if (k1 < L1 && x0 + c < G0) {
+            float2 b[L2];
+            step_b<F>(buf, tws, inv, c, k1, b);
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) {
+                const int l = k1 + L1 * k2;
+                if (in_range(l, a.out_q0, a.out_n, L)) base[(int64_t)l * a.S + c] = b[k2];
+            }
+        }
+        // the tile's buffer is loaded again two iterations on
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// per-device twiddle tables exp(-2 pi i t / L), t in [0, L), from double precision
+std::mutex g_tw_mu;
+std::map<std::pair<int, int>, float2 *> g_tw;
+
+int twiddles(int L, const float2 **out)
+{
+    int dev = 0;
+    DMR_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    auto key = std::make_pair(dev, L);
+    auto it = g_tw.find(key);
+    if (it != g_tw.end()) {
+        *out = it->second;
+        return DMR_OK;
+    }
+    std::vector<float2> h(L);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int t = 0; t < L; t++) {
+        const double ang = two_pi * (double)t / (double)L;
+        h[t] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+    }
+    float2 *d = nullptr;
+    DMR_CUDA(cudaMalloc(&d, L * sizeof(float2)));
+    DMR_CUDA(cudaMemcpy(d, h.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
+    g_tw[key] = d;
+    *out = d;
+    return DMR_OK;
+}
+
+int fft_disabled()
+{
+    static const int v = [] {
+        const char *e = getenv("DMR_CUFFT");
+        return e && atoi(e) ? 1 : 0;
+    }();
+    return v;
+}
+
+// two tiles, the twiddle table and the x apodisation (row passes)
+size_t smem_bytes(int L) { return (size_t)(2 * L * kFftLP + L) * sizeof(float2) + L * sizeof(float); }
+
+// grid size for a kernel looping over `ntiles` tiles: a few waves of resident blocks
+int blocks_for(const void *kern, int threads, size_t smem, int64_t ntiles, int *blocks)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    DMR_CUDA(cudaGetDevice(&dev));
+    DMR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    DMR_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    DMR_CHECK(per_sm >= 1, DMR_ERR_UNSUPPORTED, "FFT pass does not fit on an SM");
+    const int64_t cap = (int64_t)sms * per_sm;
+    *blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
+    return DMR_OK;
+}
+
+template <class F>
+int launch_cols_t(const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
+{
+    const size_t smem = smem_bytes(F::L);
+    const int64_t ntiles = g.nbf * a.nouter * ((g.G[0] + kFftLines - 1) / kFftLines);
+    if (ntiles == 0) return DMR_OK;
+    int blocks = 0;
+    DMR_TRY(blocks_for((const void *)fft_cols_kernel<F>, F::T, smem, ntiles, &blocks));
+    fft_cols_kernel<F><<<blocks, F::T, smem, st>>>(g, a, tw, grid);
+    DMR_LAUNCHED("fft_cols_kernel");
+    return DMR_OK;
+}
+
+template <class F, bool CROP>
+int launch_rows_t(const FftGeom &g, const float2 *tw, const void *src, int src_real, float2 *dst, cudaStream_t st)
+{
+    const size_t smem = smem_bytes(F::L);
+    const int64_t ntiles = (g.nbf * g.N[2] * g.N[1] + kFftLines - 1) / kFftLines;
+    if (ntiles == 0) return DMR_OK;
+    int blocks = 0;
+    DMR_TRY(blocks_for((const void *)fft_rows_kernel<F, CROP>, F::T, smem, ntiles, &blocks));
+    fft_rows_kernel<F, CROP><<<blocks, F::T, smem, st>>>(g, tw, src, src_real, dst);
+    DMR_LAUNCHED(CROP ? "fft_crop_rows_kernel" : "fft_pad_rows_kernel");
+    return DMR_OK;
+}
+
+int launch_cols(int L, const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
+{
+    switch (L) {
+#define DMR_FFT_CASE(L, L1, L2) case L: return launch_cols_t<Len<L, L1, L2>>(g, a, tw, grid, st);
+        DMR_FFT_LENGTHS(DMR_FFT_CASE)
+#undef DMR_FFT_CASE
+    default: return DMR_ERR_UNSUPPORTED;
+    }
+}
+
+int launch_rows(int L, bool crop, const FftGeom &g, const float2 *tw, const void *src, int src_real, float2 *dst,
+                cudaStream_t st)
+{
+    switch (L) {
+#define DMR_FFT_CASE(L, L1, L2)                                                                     \
+    case L:                                                                                         \
+        return crop ? launch_rows_t<Len<L, L1, L2>, true>(g, tw, src, src_real, dst, st)            \
+                    : launch_rows_t<Len<L, L1, L2>, false>(g, tw, src, src_real, dst, st);
+        DMR_FFT_LENGTHS(DMR_FFT_CASE)
+#undef DMR_FFT_CASE
+    default: return DMR_ERR_UNSUPPORTED;
+    }
+}
+
+FftGeom make_geom(const dmr_plan *p, int64_t batch, float scale)
+{
+    const Geom &gg = p->g;
+    FftGeom g;
+    for (int a = 0; a < 3; a++) {
+        g.N[a] = gg.N[a];
+        g.G[a] = gg.G[a];
+        g.apod[a] = gg.W[a] != 1 ? p->apod[a] : nullptr;
+    }
+    g.nbf = batch * gg.nframes;
+    g.gsize = gg.gsize;
+    g.isize = gg.isize;
+    g.scale = scale;
+    return g;
+}
+
+ColArgs y_pass(const FftGeom &g, bool inv)
+{
+    // y columns of the N2 planes that hold data; the forward reads the N1
+    // valid y only, the adjoint writes the N1 kept y only
+    ColArgs a;
+    a.S = g.G[0];
+    a.outer_stride = (int64_t)g.G[0] * g.G[1];
+    a.nouter = g.N[2];
+    a.outer_q0 = wrapi(-(g.N[2] / 2), g.G[2]);
+    a.outer_G = g.G[2];
+    const int q0 = wrapi(-(g.N[1] / 2), g.G[1]);
+    a.in_q0 = inv ? 0 : q0;
+    a.in_n = inv ? g.G[1] : g.N[1];
+    a.out_q0 = inv ? q0 : 0;
+    a.out_n = inv ? g.N[1] : g.G[1];
+    a.inv = inv;
+    return a;
+}
+
+ColArgs z_pass(const FftGeom &g, bool inv)
+{
+    // z columns of every (y, x); the forward reads the N2 valid z only, the
+    // adjoint writes the N2 kept z only
+    ColArgs a;
+    a.S = (int64_t)g.G[0] * g.G[1];
+    a.outer_stride = g.G[0];
+    a.nouter = g.G[1];
+    a.outer_q0 = 0;
+    a.outer_G = g.G[1];
+    const int q0 = wrapi(-(g.N[2] / 2), g.G[2]);
+    a.in_q0 = inv ? 0 : q0;
+    a.in_n = inv ? g.G[2] : g.N[2];
+    a.out_q0 = inv ? q0 : 0;
+    a.out_n = inv ? g.N[2] : g.G[2];
+    a.inv = inv;
+    return a;
+}
+
+}  // namespace
+
+bool fft3_applies(const dmr_plan *p)
+{
+    const Geom &g = p->g;
+    if (fft_disabled() || g.ndim != 3) return false;
+    for (int a = 0; a < 3; a++)
+        if (g.G[a] < g.N[a] || !has_len(g.G[a])) return false;
+    return true;
+}
+
+// apodise + zero-pad + forward 3D FFT of `image` into `grid` (FFT order)
+int fft3_forward(const dmr_plan *p, const void *image, int image_real, int64_t batch, float2 *grid,
+                 cudaStream_t st)
+{
+    const FftGeom g = make_geom(p, batch, 1.0f);
+    const float2 *tw[3];
+    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    if (g.nbf == 0) return DMR_OK;
+    DMR_TRY(launch_rows(g.G[0], false, g, tw[0], image, image_real, grid, st));
+    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, false), tw[1], grid, st));
+    return launch_cols(g.G[2], g, z_pass(g, false), tw[2], grid, st);
+}
+
+// inverse 3D FFT of `grid` (FFT order, overwritten) + crop + 1/G + apodisation into `image`
+int fft3_adjoint(const dmr_plan *p, float2 *grid, int64_t batch, float2 *image, cudaStream_t st)
+{
+    const FftGeom g = make_geom(p, batch, (float)(1.0 / (double)p->g.gsize));
+    const float2 *tw[3];
+    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    if (g.nbf == 0) return DMR_OK;
+    DMR_TRY(launch_cols(g.G[2], g, z_pass(g, true), tw[2], grid, st));
+    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], grid, st));
+    return launch_rows(g.G[0], true, g, tw[0], grid, 0, image, st);
+}
+
+}  // namespace dmr
+
+extern "C" int dmr_fft3_fused(dmr_plan *plan) { return plan && dmr::fft3_applies(plan) ? 1 : 0; }

@@ -182,13 +182,17 @@ struct NufftWs {
 static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, NufftWs &out, size_t *need)
 {
     const Geom &g = p->g;
-    int dims[3];
-    zyx_dims(g, g.G, dims);
-    int err = DMR_OK;
-    auto fp = get_fft_plan(g.ndim, dims, batch * g.nframes, &err);
-    if (!fp) return err;
+    // the fused FFT passes need no cuFFT plan or work area
+    std::shared_ptr<FftPlan> fp;
+    if (!fft3_applies(p)) {
+        int dims[3];
+        zyx_dims(g, g.G, dims);
+        int err = DMR_OK;
+        fp = get_fft_plan(g.ndim, dims, batch * g.nframes, &err);
+        if (!fp) return err;
+    }
     const size_t grid_bytes = align_up((size_t)batch * g.nframes * g.gsize * sizeof(float2), 256);
-    const size_t fft_bytes = align_up(fp->work_bytes, 256);
+    const size_t fft_bytes = fp ? align_up(fp->work_bytes, 256) : 0;
     const size_t rt_bytes = align_up(grid_scratch_bytes(p, batch), 256);
     const size_t total = grid_bytes + fft_bytes + rt_bytes;
     if (need) *need = total;
@@ -196,7 +200,7 @@ static int nufft_ws(dmr_plan *p, int64_t batch, void *ws, size_t ws_bytes, Nufft
     DMR_CHECK(ws_bytes >= total, DMR_ERR_WORKSPACE, "workspace too small: %zu < %zu", ws_bytes, total);
     DMR_CHECK(((uintptr_t)ws & 255) == 0, DMR_ERR_INVALID, "workspace must be 256-byte aligned");
     out.grid = (float2 *)ws;
-    out.fft_work = fp->work_bytes ? (char *)ws + grid_bytes : nullptr;
+    out.fft_work = fp && fp->work_bytes ? (char *)ws + grid_bytes : nullptr;
     out.rt_scratch = rt_bytes ? (char *)ws + grid_bytes + fft_bytes : nullptr;
     out.rt_bytes = rt_bytes;
     out.fft = fp;
@@ -331,6 +335,11 @@ int forward_grid(dmr_plan *p, const void *image, int image_real, int64_t batch, 
     const Geom &g = p->g;
     NufftWs w;
     DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
+    if (!w.fft) {
+        DMR_TRY(fft3_forward(p, image, image_real, batch, w.grid, st));
+        *grid_out = w.grid;
+        return DMR_OK;
+    }
     ResizeArgs r;
     memset(&r, 0, sizeof(r));
     for (int a = 0; a < 3; a++) {
@@ -378,6 +387,7 @@ extern "C" int dmr_nufft_adjoint(dmr_plan *p, const void *kspace, int kspace_rea
     DMR_TRY(nufft_ws(p, batch, workspace, workspace_bytes, w, nullptr));
     DMR_TRY(grid_dispatch(p, kspace, kspace_real, w.grid, batch, weight, weight_per_batch,
                           deterministic, w.rt_scratch, w.rt_bytes, st));
+    if (!w.fft) return fft3_adjoint(p, w.grid, batch, (float2 *)image, st);
     DMR_TRY(fft_exec(*w.fft, w.grid, CUFFT_INVERSE, w.fft_work, st));
     ResizeArgs r;
     memset(&r, 0, sizeof(r));

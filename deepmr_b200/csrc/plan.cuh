@@ -80,6 +80,15 @@ size_t tm_scratch_bytes(const ::dmr_plan *p, int64_t batch);
 size_t grid_scratch_bytes(const ::dmr_plan *p, int64_t batch);
 // library-owned stream-ordered pool for the scratch of calls without a workspace
 cudaMemPool_t scratch_pool(int dev);
+// fused, pruned 3D FFT passes of the NUFFT pipelines (fftpass.cu): whether they
+// apply to the plan (3D, every grid extent at least the image's, at most 512
+// and a product of 2, 3 and 5; DMR_CUFFT=1 turns them off), the forward
+// (apodise + pad + FFT into the grid) and the adjoint (inverse FFT of the grid,
+// which it overwrites, + crop + 1/G + apodisation into the image)
+bool fft3_applies(const ::dmr_plan *p);
+int fft3_forward(const ::dmr_plan *p, const void *image, int image_real, int64_t batch, float2 *grid,
+                 cudaStream_t st);
+int fft3_adjoint(const ::dmr_plan *p, float2 *grid, int64_t batch, float2 *image, cudaStream_t st);
 // tensor-core atomic gridding of 3D plans (tcgrid.cu); DMR_ERR_UNSUPPORTED when
 // the bin region does not fit
 int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,

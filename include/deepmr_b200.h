@@ -87,6 +87,16 @@ int dmr_plan_status(dmr_plan *plan, int32_t *failed, int reset, void *stream);
 int dmr_tc_test_stall(int enable);
 
 /*
+ * Query, no reference counterpart: 1 if the plan's forward / adjoint NUFFT
+ * run their 3D FFT as the library's fused passes (apodise + zero-pad + FFT,
+ * inverse FFT + crop + 1/G + apodisation, pruned to the lines with data),
+ * 0 if they use cuFFT with separate pad / crop kernels (grid extents without
+ * a compiled transform, 1D / 2D plans, or DMR_CUFFT=1 in the environment).
+ * Replaces the FFT step of src/deepmr/fft/nufft.py:502-505 and 583-590.
+ */
+int dmr_fft3_fused(dmr_plan *plan);
+
+/*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
  * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
  * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the
