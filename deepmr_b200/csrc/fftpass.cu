@@ -37,13 +37,24 @@ namespace dmr {
 
 namespace {
 
-constexpr int kFftLines = 16;  // lines per block
-constexpr int kFftLP = 17;     // shared-memory pitch of a position (lines + 1)
+#ifndef DMR_FFT_LINES
+#define DMR_FFT_LINES 16
+#endif
+#ifndef DMR_FFT_MINB
+#define DMR_FFT_MINB 2
+#endif
+constexpr int kFftLines = DMR_FFT_LINES;  // lines per block (16 or 32)
+constexpr int kFftLP = kFftLines + 2;     // shared-memory pitch of a position (16-byte rows)
+constexpr int kFftShift = kFftLines == 32 ? 5 : 4;
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+
+// complex add / subtract as packed FP32 (one instruction each)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
 
 // R-point DFT of v in place, V[m] = sum_q v[q] w^(q m), w = exp(-+2 pi i / R),
 // for R = 2, 4 (no multiplications), 3 and 5 (roots of unity from the table
@@ -53,19 +64,17 @@ __device__ __forceinline__ void small_dft(float2 *v, const float2 *tw, bool inv)
 {
     if constexpr (R == 2) {
         const float2 a = v[0], b = v[1];
-        v[0] = make_float2(a.x + b.x, a.y + b.y);
-        v[1] = make_float2(a.x - b.x, a.y - b.y);
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
     } else if constexpr (R == 4) {
-        const float2 s02 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
-        const float2 d02 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
-        const float2 s13 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
-        const float2 d13 = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
+        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const float2 s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
         // w d13 with w = -i (forward) or +i (inverse)
         const float2 jd = inv ? make_float2(-d13.y, d13.x) : make_float2(d13.y, -d13.x);
-        v[0] = make_float2(s02.x + s13.x, s02.y + s13.y);
-        v[1] = make_float2(d02.x + jd.x, d02.y + jd.y);
-        v[2] = make_float2(s02.x - s13.x, s02.y - s13.y);
-        v[3] = make_float2(d02.x - jd.x, d02.y - jd.y);
+        v[0] = cadd(s02, s13);
+        v[1] = cadd(d02, jd);
+        v[2] = csub(s02, s13);
+        v[3] = csub(d02, jd);
     } else if constexpr (R == 3) {
         // w^2 = conj(w): V1,2 = v0 + Re(w) (v1 + v2) +- i Im(w) (v1 - v2)
         float2 w = tw[L / 3];
@@ -163,20 +172,35 @@ struct Len {
 // ([position][line]): line c, column n2 takes positions L2 n1 + n2, an
 // L1-point DFT, twiddles w_L^(n2 k1), back to positions L2 k1 + n2 (the
 // positions it read: no barrier needed between its reads and writes).
+// With `scale` the inputs are first multiplied by scale_line[c] * scale[position].
 template <class F>
-__device__ __forceinline__ void step_a(float2 *buf, const float2 *tw, bool inv)
+__device__ __forceinline__ void step_a(float2 *buf, const float2 *tw, bool inv, const float *scale = nullptr,
+                                       const float *scale_line = nullptr)
 {
     constexpr int L = F::L, L1 = F::L1, L2 = F::L2;
     const int w = threadIdx.x;
     if (w < kFftLines * L2) {
-        const int c = w & (kFftLines - 1), n2 = w >> 4;
+        const int c = w & (kFftLines - 1), n2 = w >> kFftShift;
         float2 a[L1];
 #pragma unroll
         for (int n1 = 0; n1 < L1; n1++) a[n1] = buf[(L2 * n1 + n2) * kFftLP + c];
+        if (scale) {
+            const float sl = scale_line[c];
+#pragma unroll
+            for (int n1 = 0; n1 < L1; n1++) {
+                const float sc = sl * scale[L2 * n1 + n2];
+                a[n1].x *= sc;
+                a[n1].y *= sc;
+            }
+        }
         reg_dft<L1, L>(a, tw, inv);
+        // twiddles w_L^(n2 k1), index n2 k1 mod L kept incrementally
+        int ti = 0;
 #pragma unroll
         for (int k1 = 1; k1 < L1; k1++) {
-            float2 t = tw[(n2 * k1) % L];
+            ti += n2;
+            if (ti >= L) ti -= L;
+            float2 t = tw[ti];
             if (inv) t.y = -t.y;
             a[k1] = cmulf(a[k1], t);
         }
@@ -295,7 +319,7 @@ __device__ __forceinline__ void row_lines(const FftGeom &g, int64_t row0, int64_
 //   adjoint (CROP true): grid rows are inverse-transformed and the kept x,
 //   scaled and apodised, written to the image.
 template <class F, bool CROP>
-__global__ void __launch_bounds__(F::T) fft_rows_kernel(FftGeom g, const float2 *__restrict__ tw,
+__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_rows_kernel(FftGeom g, const float2 *__restrict__ tw,
                                                         const void *__restrict__ src, int src_real,
                                                         float2 *__restrict__ dst)
 {
@@ -303,19 +327,29 @@ __global__ void __launch_bounds__(F::T) fft_rows_kernel(FftGeom g, const float2 
     extern __shared__ __align__(16) float2 fsm[];
     float2 *bufs = fsm;                               // 2 x L * 17
     float2 *tws = fsm + 2 * L * kFftLP;               // L
-    float *apx = reinterpret_cast<float *>(tws + L);  // L: x apodisation by image index
+    // L floats: the forward pass's x apodisation by grid position q (zero
+    // outside the image), the adjoint's by image index i
+    float *apx = reinterpret_cast<float *>(tws + L);
     __shared__ RowLine lines[2][kFftLines];
+    __shared__ float line_s[2][kFftLines];
+    const int N0 = g.N[0], h0 = N0 / 2;
     for (int i = threadIdx.x; i < L; i += T) {
         tws[i] = tw[i];
-        apx[i] = (g.apod[0] && i < g.N[0]) ? g.apod[0][i] : 1.0f;
+        if (CROP) {
+            apx[i] = (g.apod[0] && i < N0) ? g.apod[0][i] : 1.0f;
+        } else {
+            int ii = i + h0;
+            if (ii >= L) ii -= L;
+            apx[i] = ii < N0 ? (g.apod[0] ? g.apod[0][ii] : 1.0f) : 0.0f;
+        }
     }
-    const int N0 = g.N[0], h0 = N0 / 2;
     const int64_t nrows = g.nbf * g.N[2] * g.N[1];
     const int64_t ntiles = (nrows + kFftLines - 1) / kFftLines;
     // loads of tile t into buffer `slot` (line data first, so a barrier)
     auto prefetch = [&](int64_t t, int slot) {
         row_lines(g, t * kFftLines, nrows, lines[slot]);
         __syncthreads();
+        if (threadIdx.x < kFftLines) line_s[slot][threadIdx.x] = lines[slot][threadIdx.x].s;
         float2 *buf = bufs + slot * L * kFftLP;
         for (int e = threadIdx.x; e < kFftLines * L; e += T) {
             const int c = e / L, q = e - c * L;
@@ -348,25 +382,15 @@ __global__ void __launch_bounds__(F::T) fft_rows_kernel(FftGeom g, const float2 
         else cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
-        if (!CROP) {
-            // apodisation: position q of line c holds image index (q + N0/2) mod L, or zero
-            for (int e = threadIdx.x; e < kFftLines * L; e += T) {
-                const int q = e >> 4, c = e & (kFftLines - 1);
-                int i = q + h0;
-                if (i >= L) i -= L;
-                const float sc = lines[cur][c].s * (i < N0 ? apx[i] : 0.0f);
-                float2 &v = buf[q * kFftLP + c];
-                v.x *= sc;
-                v.y *= sc;
-            }
-            __syncthreads();
-        }
-        step_a<F>(buf, tws, CROP);
+        // forward: apodisation (position q of line c holds image index
+        // (q + N0/2) mod L, or zero) applied as step A reads its inputs
+        if (CROP) step_a<F>(buf, tws, true);
+        else step_a<F>(buf, tws, false, apx, line_s[cur]);
         __syncthreads();
         // step B into registers, then (after every thread has read its
         // inputs) back into the tile in transform order
         const int w = threadIdx.x;
-        const int c = w & (kFftLines - 1), k1 = w >> 4;
+        const int c = w & (kFftLines - 1), k1 = w >> kFftShift;
         float2 b[L2];
         if (k1 < L1) step_b<F>(buf, tws, CROP, c, k1, b);
         __syncthreads();
@@ -416,8 +440,8 @@ struct ColArgs {
     int inv;
 };
 
-template <class F>
-__global__ void __launch_bounds__(F::T) fft_cols_kernel(FftGeom g, ColArgs a, const float2 *__restrict__ tw,
+template <class F, bool IN_ALL, bool OUT_ALL>
+__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_cols_kernel(FftGeom g, ColArgs a, const float2 *__restrict__ tw,
                                                         float2 *grid)
 {
     constexpr int L = F::L, L1 = F::L1, L2 = F::L2, T = F::T;
@@ -443,10 +467,16 @@ __global__ void __launch_bounds__(F::T) fft_cols_kernel(FftGeom g, ColArgs a, co
         int x0;
         const float2 *base = tile(t, x0);
         float2 *buf = bufs + slot * L * kFftLP;
-        for (int e = threadIdx.x; e < kFftLines * L; e += T) {
-            const int l = e >> 4, c = e & (kFftLines - 1);
-            const bool ok = x0 + c < G0 && in_range(l, a.in_q0, a.in_n, L);
-            cp_async_fill(buf + l * kFftLP + c, ok ? base + (int64_t)l * a.S + c : base, 8, ok);
+        // pairs of x (16 bytes; grid extents are even, so a pair never
+        // straddles the end of a row)
+        constexpr int P = kFftLines / 2;
+        for (int e = threadIdx.x; e < P * L; e += T) {
+            const int l = e / P, c = 2 * (e - l * P);
+            const bool ok = x0 + c < G0 && (IN_ALL || in_range(l, a.in_q0, a.in_n, L));
+            const unsigned d = (unsigned)__cvta_generic_to_shared(buf + l * kFftLP + c);
+            const float2 *sp = ok ? base + (int64_t)l * a.S + c : base;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(sp), "r"(ok ? 16 : 0)
+                         : "memory");
         }
         cp_async_commit();
     };
@@ -462,7 +492,7 @@ __global__ void __launch_bounds__(F::T) fft_cols_kernel(FftGeom g, ColArgs a, co
         step_a<F>(buf, tws, inv);
         __syncthreads();
         const int w = threadIdx.x;
-        const int c = w & (kFftLines - 1), k1 = w >> 4;
+        const int c = w & (kFftLines - 1), k1 = w >> kFftShift;
         int x0;
         float2 *base = tile(t, x0);
         if (k1 < L1 && x0 + c < G0) {
@@ -471,7 +501,7 @@ __global__ void __launch_bounds__(F::T) fft_cols_kernel(FftGeom g, ColArgs a, co
 #pragma unroll
             for (int k2 = 0; k2 < L2; k2++) {
                 const int l = k1 + L1 * k2;
-                if (in_range(l, a.out_q0, a.out_n, L)) base[(int64_t)l * a.S + c] = b[k2];
+                if (OUT_ALL || in_range(l, a.out_q0, a.out_n, L)) base[(int64_t)l * a.S + c] = b[k2];
             }
         }
         // the tile's buffer is loaded again two iterations on
@@ -535,17 +565,28 @@ int blocks_for(const void *kern, int threads, size_t smem, int64_t ntiles, int *
     return DMR_OK;
 }
 
-template <class F>
-int launch_cols_t(const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
+template <class F, bool IN_ALL, bool OUT_ALL>
+int launch_cols_tt(const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
 {
     const size_t smem = smem_bytes(F::L);
     const int64_t ntiles = g.nbf * a.nouter * ((g.G[0] + kFftLines - 1) / kFftLines);
     if (ntiles == 0) return DMR_OK;
     int blocks = 0;
-    DMR_TRY(blocks_for((const void *)fft_cols_kernel<F>, F::T, smem, ntiles, &blocks));
-    fft_cols_kernel<F><<<blocks, F::T, smem, st>>>(g, a, tw, grid);
+    DMR_TRY(blocks_for((const void *)fft_cols_kernel<F, IN_ALL, OUT_ALL>, F::T, smem, ntiles, &blocks));
+    fft_cols_kernel<F, IN_ALL, OUT_ALL><<<blocks, F::T, smem, st>>>(g, a, tw, grid);
     DMR_LAUNCHED("fft_cols_kernel");
     return DMR_OK;
+}
+
+// the forward passes read part of each line and write all of it, the
+// adjoint passes the other way round
+template <class F>
+int launch_cols_t(const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
+{
+    const int L = F::L;
+    if (a.out_n == L) return launch_cols_tt<F, false, true>(g, a, tw, grid, st);
+    if (a.in_n == L) return launch_cols_tt<F, true, false>(g, a, tw, grid, st);
+    return launch_cols_tt<F, false, false>(g, a, tw, grid, st);
 }
 
 template <class F, bool CROP>
