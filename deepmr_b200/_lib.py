@@ -35,6 +35,7 @@ SYMBOLS = (
     "dmr_plan_status",
     "dmr_tc_test_stall",
     "dmr_fft3_fused",
+    "dmr_tc_min_coils",
     "dmr_detect_cartesian",
     "dmr_plan_create",
     "dmr_plan_destroy",
@@ -88,6 +89,7 @@ _SIGS = {
     "dmr_plan_status": (ctypes.c_int, [vp, i32p, ctypes.c_int, vp]),
     "dmr_tc_test_stall": (ctypes.c_int, [ctypes.c_int]),
     "dmr_fft3_fused": (ctypes.c_int, [vp]),
+    "dmr_tc_min_coils": (ctypes.c_int, [ctypes.c_int]),
     "dmr_detect_cartesian": (ctypes.c_int, [vp, i64, ctypes.c_int, i32p, i32p, vp]),
     "dmr_plan_create": (
         ctypes.c_int,

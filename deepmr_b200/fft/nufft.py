@@ -612,10 +612,11 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
             )
         )
 
-    # the 3D tensor-core gridding costs about the same for 8 coils as for 32
-    # (the spreading weights are built once per sample and launch), so the
-    # adjoint's chunks keep at least 8 batch items
-    min_chunk = 8 if nufft_plan.ndim == 3 else 1
+    # chunks of a 3D adjoint: atomic gridding of a few coils runs on the CUDA
+    # cores at a cost proportional to the coils, so 4 per chunk; the
+    # deterministic tensor-core gridding costs about the same for 8 coils as
+    # for 32, so at least 8
+    min_chunk = (8 if det else 4) if nufft_plan.ndim == 3 else 1
     if batch >= 2 * min_chunk and _pipelinable(kspace, dev, batch, 8 * int(np.prod(item))):
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
         out = torch.empty([batch] + item, dtype=torch.complex64, pin_memory=True)

@@ -97,6 +97,15 @@ int dmr_tc_test_stall(int enable);
 int dmr_fft3_fused(dmr_plan *plan);
 
 /*
+ * Tuning knob, no reference counterpart: atomic gridding of a 3D plan runs on
+ * the tensor cores for batches of at least `coils` coils (default 20; below,
+ * the CUDA-core kernel, whose cost scales with the coil count, is faster) and
+ * on the CUDA cores otherwise. coils <= 0 only queries. Returns the previous
+ * value. Process-wide; deterministic gridding is not affected.
+ */
+int dmr_tc_min_coils(int coils);
+
+/*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
  * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
  * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the

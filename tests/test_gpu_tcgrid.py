@@ -26,9 +26,14 @@ def rel(a, b):
 
 @pytest.fixture(scope="module")
 def F():
+    """The fft module, with atomic 3D gridding on the tensor cores for every
+    coil count (by default batches under 20 coils run on the CUDA cores)."""
     import deepmr_b200.fft as F
+    from deepmr_b200 import _lib
 
-    return F
+    old = _lib.lib().dmr_tc_min_coils(1)
+    yield F
+    _lib.lib().dmr_tc_min_coils(old)
 
 
 def _grid(F, plan, ksp, weight=None, det=False):
