@@ -58,12 +58,16 @@ namespace dmr {
 
 namespace {
 
-constexpr int kTmBuilders = 256;           // warps 0-7: two groups of 128 threads, alternate chunks
+#ifndef DMR_TM_BUILDER_GROUPS
+#define DMR_TM_BUILDER_GROUPS 3
+#endif
+constexpr int kTmGroups = DMR_TM_BUILDER_GROUPS;  // builder groups of 128 threads, chunks in turn
 constexpr int kTmGroup = 128;
-constexpr int kTmEpiWarp = 8;              // warps 8-15 (two per tensor-memory lane quarter)
-constexpr int kTmMmaWarp = 16;
-constexpr int kTmValueWarp = 17;
-constexpr int kTmThreads = 18 * 32;
+constexpr int kTmBuilders = kTmGroups * kTmGroup;  // warps 0 .. 4 groups - 1
+constexpr int kTmEpiWarp = 4 * kTmGroups;          // 8 read-back warps (two per tensor-memory lane quarter)
+constexpr int kTmMmaWarp = kTmEpiWarp + 8;
+constexpr int kTmValueWarp = kTmMmaWarp + 1;
+constexpr int kTmThreads = (kTmValueWarp + 1) * 32;
 constexpr int kTmEpi = 256;
 constexpr int kTmMaxRows = 24;             // region rows over the three axes (7 + 6 + 6 = 19 used)
 constexpr int kTmTable = kTmMaxRows * 8;   // a chunk's weight table: rows x 8 samples
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
         for (int i = 0; i < kBarCount; i++) {
             int c = 1;  // commits and the final / test barriers
             if (i < kBarPassEmpty) c = kTmPassArrivals;
-            else if (i < kBarStFull) c = kTmBuilders;   // pass empty: both builder groups
+            else if (i < kBarStFull) c = kTmBuilders;   // pass empty: every builder group
             else if (i < kBarStEmpty) c = kTmGroup;     // stage full: the group that built the chunk
             else if (i >= kBarAccEmpty && i < kBarFinal) c = kTmEpi;
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar_addr(bars, i)), "r"(c));
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             for (int ch = 0; ch < nch; ch++) {
                 const bool first = (flags & kPassFirst) && ch == 0;
                 const bool last = (flags & kPassLast) && ch == nch - 1;
-                if ((int)(chunk_no & 1) != bg) {
+                if ((int)(chunk_no % kTmGroups) != bg) {
                     // the other group builds this chunk
                     chunk_no++;
                     if (last) task_no++;
@@ -370,7 +374,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                 // the chunk's weight table: Kaiser-Bessel weight of sample s at region
                 // row r of each axis (zero off its taps); two per group, alternating
                 // (a table is written again only after the group's next barrier)
-                float *table = tables + ((chunk_no >> 1) & 1) * kTmTable;
+                float *table = tables + ((chunk_no / kTmGroups) & 1) * kTmTable;
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int e = btid + 128 * h;
@@ -442,7 +446,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             if (!ok) break;
             bar_arrive(bar_addr(bars, kBarPassEmpty + slot));
         }
-        if (ok && (int)(chunk_no & 1) == bg) {
+        if (ok && (int)(chunk_no % kTmGroups) == bg) {
             // end marker for the MMA thread, from the group whose turn it is
             const int stage = chunk_no % sh.nstages;
             if (chunk_no < (uint32_t)sh.nstages ||
@@ -757,7 +761,7 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
             const int stages_off = (ns * s.slot_bytes + 1023) / 1024 * 1024;
             const int x_off = stages_off + nst * kTmStageBytes;
             const int table_off = x_off + kTmXBytes;
-            const int goff_off = table_off + 4 * kTmTable * 4;
+            const int goff_off = table_off + 2 * kTmGroups * kTmTable * 4;
             if (goff_off + kTmN * 4 <= smem_limit) {
                 s.nslots = ns;
                 s.nstages = nst;
