@@ -239,6 +239,7 @@ bool has_len(int L)
 
 struct FftGeom {
     int N[3], G[3];       // image / grid extents (x, y, z)
+    int off[3];           // image index i sits at grid position (i + off) mod G
     int64_t nbf;          // batch * frames
     int64_t gsize, isize; // points per grid / image
     const float *apod[3]; // per-axis apodisation by image index (nullptr: 1)
@@ -299,7 +300,7 @@ __device__ __forceinline__ void row_lines(const FftGeom &g, int64_t row0, int64_
         const int64_t bf = row / plane;
         const int rr = (int)(row - bf * plane);
         const int y = rr % N1, z = rr / N1;
-        const int qy = wrapi(y - N1 / 2, g.G[1]), qz = wrapi(z - N2 / 2, g.G[2]);
+        const int qy = wrapi(y + g.off[1], g.G[1]), qz = wrapi(z + g.off[2], g.G[2]);
         ln.img = bf * g.isize + (int64_t)rr * g.N[0];
         ln.grid = bf * g.gsize + ((int64_t)qz * g.G[1] + qy) * g.G[0];
         float s = g.scale;
@@ -332,7 +333,8 @@ __global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_rows_kernel(FftGeom g,
     float *apx = reinterpret_cast<float *>(tws + L);
     __shared__ RowLine lines[2][kFftLines];
     __shared__ float line_s[2][kFftLines];
-    const int N0 = g.N[0], h0 = N0 / 2;
+    // h0: grid position q holds image index (q + h0) mod L (when below N0)
+    const int N0 = g.N[0], h0 = wrapi(-g.off[0], L);
     for (int i = threadIdx.x; i < L; i += T) {
         tws[i] = tw[i];
         if (CROP) {
@@ -510,6 +512,103 @@ __global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_cols_kernel(FftGeom g,
     cp_async_wait<0>();
 }
 
+// Toeplitz z pass: per tile of 16 x of one (batch, y), the z columns (reading
+// the N2 z with data only), forward FFT, times kernel[b mod nk][z][y][x] *
+// kscale, inverse FFT, and the N2 kept z written back; nothing leaves shared
+// memory between the two transforms. Tiles run batch-fastest, so the blocks
+// that read one kernel tile run together and share it in L2.
+template <class F>
+__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_toep_z_kernel(FftGeom g, ColArgs a, int64_t nk,
+                                                          const float2 *__restrict__ kern, float kscale,
+                                                          const float2 *__restrict__ tw, float2 *grid)
+{
+    constexpr int L = F::L, L1 = F::L1, L2 = F::L2, T = F::T;
+    extern __shared__ __align__(16) float2 fsm[];
+    float2 *bufs = fsm, *tws = fsm + 2 * L * kFftLP;
+    for (int i = threadIdx.x; i < L; i += T) tws[i] = tw[i];
+    const int G0 = g.G[0];
+    const int ntx = (G0 + kFftLines - 1) / kFftLines;
+    const int64_t ntiles = g.nbf * a.nouter * ntx;
+    // batch index, first x, and the tile's offset in a grid (y row a.outer)
+    auto tile = [&](int64_t t, int64_t &bf, int &x0) -> int64_t {
+        bf = t % g.nbf;
+        const int64_t rest = t / g.nbf;
+        const int tx = (int)(rest % ntx);
+        const int k = (int)(rest / ntx);
+        x0 = tx * kFftLines;
+        return (int64_t)k * a.outer_stride + x0;
+    };
+    auto prefetch = [&](int64_t t, int slot) {
+        int64_t bf;
+        int x0;
+        const float2 *base = grid + tile(t, bf, x0) + bf * g.gsize;
+        float2 *buf = bufs + slot * L * kFftLP;
+        constexpr int P = kFftLines / 2;
+        for (int e = threadIdx.x; e < P * L; e += T) {
+            const int l = e / P, c = 2 * (e - l * P);
+            const bool ok = x0 + c < G0 && in_range(l, a.in_q0, a.in_n, L);
+            const unsigned d = (unsigned)__cvta_generic_to_shared(buf + l * kFftLP + c);
+            const float2 *sp = ok ? base + (int64_t)l * a.S + c : base;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(sp), "r"(ok ? 16 : 0)
+                         : "memory");
+        }
+        cp_async_commit();
+    };
+    int64_t t = blockIdx.x;
+    if (t < ntiles) prefetch(t, 0);
+    for (int it = 0; t < ntiles; t += gridDim.x, it++) {
+        const int cur = it & 1;
+        float2 *buf = bufs + cur * L * kFftLP;
+        if (t + gridDim.x < ntiles) prefetch(t + gridDim.x, cur ^ 1);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        int64_t bf;
+        int x0;
+        const int64_t to = tile(t, bf, x0);
+        const int w = threadIdx.x;
+        const int c = w & (kFftLines - 1), k1 = w >> kFftShift;
+        // forward transform back into the tile (transform order)
+        step_a<F>(buf, tws, false);
+        __syncthreads();
+        float2 b[L2];
+        if (k1 < L1) step_b<F>(buf, tws, false, c, k1, b);
+        __syncthreads();
+        if (k1 < L1) {
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) buf[(k1 + L1 * k2) * kFftLP + c] = b[k2];
+        }
+        __syncthreads();
+        // kernel multiply
+        const float2 *kb = kern + (bf % nk) * g.gsize + to;
+        for (int e = threadIdx.x; e < kFftLines * L; e += T) {
+            const int l = e >> kFftShift, cc = e & (kFftLines - 1);
+            if (x0 + cc < G0) {
+                const float2 kv = kb[(int64_t)l * a.S + cc];
+                float2 &v = buf[l * kFftLP + cc];
+                const float2 m = cmulf(kv, v);
+                v = make_float2(m.x * kscale, m.y * kscale);
+            }
+        }
+        __syncthreads();
+        // inverse transform, kept z to the grid
+        step_a<F>(buf, tws, true);
+        __syncthreads();
+        if (k1 < L1 && x0 + c < G0) {
+            step_b<F>(buf, tws, true, c, k1, b);
+            float2 *base = grid + bf * g.gsize + to;
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) {
+                const int l = k1 + L1 * k2;
+                if (in_range(l, a.out_q0, a.out_n, L)) base[(int64_t)l * a.S + c] = b[k2];
+            }
+        }
+        // the tile's buffer is loaded again two iterations on
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
 // per-device twiddle tables exp(-2 pi i t / L), t in [0, L), from double precision
 std::mutex g_tw_mu;
 std::map<std::pair<int, int>, float2 *> g_tw;
@@ -602,6 +701,31 @@ int launch_rows_t(const FftGeom &g, const float2 *tw, const void *src, int src_r
     return DMR_OK;
 }
 
+template <class F>
+int launch_toep_z_t(const FftGeom &g, const ColArgs &a, int64_t nk, const float2 *kern, float kscale,
+                    const float2 *tw, float2 *grid, cudaStream_t st)
+{
+    const size_t smem = smem_bytes(F::L);
+    const int64_t ntiles = g.nbf * a.nouter * ((g.G[0] + kFftLines - 1) / kFftLines);
+    if (ntiles == 0) return DMR_OK;
+    int blocks = 0;
+    DMR_TRY(blocks_for((const void *)fft_toep_z_kernel<F>, F::T, smem, ntiles, &blocks));
+    fft_toep_z_kernel<F><<<blocks, F::T, smem, st>>>(g, a, nk, kern, kscale, tw, grid);
+    DMR_LAUNCHED("fft_toep_z_kernel");
+    return DMR_OK;
+}
+
+int launch_toep_z(int L, const FftGeom &g, const ColArgs &a, int64_t nk, const float2 *kern, float kscale,
+                  const float2 *tw, float2 *grid, cudaStream_t st)
+{
+    switch (L) {
+#define DMR_FFT_CASE(L, L1, L2) case L: return launch_toep_z_t<Len<L, L1, L2>>(g, a, nk, kern, kscale, tw, grid, st);
+        DMR_FFT_LENGTHS(DMR_FFT_CASE)
+#undef DMR_FFT_CASE
+    default: return DMR_ERR_UNSUPPORTED;
+    }
+}
+
 int launch_cols(int L, const FftGeom &g, const ColArgs &a, const float2 *tw, float2 *grid, cudaStream_t st)
 {
     switch (L) {
@@ -634,6 +758,7 @@ FftGeom make_geom(const dmr_plan *p, int64_t batch, float scale)
         g.N[a] = gg.N[a];
         g.G[a] = gg.G[a];
         g.apod[a] = gg.W[a] != 1 ? p->apod[a] : nullptr;
+        g.off[a] = -(gg.N[a] / 2);  // FFT order: centred index N/2 at 0
     }
     g.nbf = batch * gg.nframes;
     g.gsize = gg.gsize;
@@ -650,9 +775,9 @@ ColArgs y_pass(const FftGeom &g, bool inv)
     a.S = g.G[0];
     a.outer_stride = (int64_t)g.G[0] * g.G[1];
     a.nouter = g.N[2];
-    a.outer_q0 = wrapi(-(g.N[2] / 2), g.G[2]);
+    a.outer_q0 = wrapi(g.off[2], g.G[2]);
     a.outer_G = g.G[2];
-    const int q0 = wrapi(-(g.N[1] / 2), g.G[1]);
+    const int q0 = wrapi(g.off[1], g.G[1]);
     a.in_q0 = inv ? 0 : q0;
     a.in_n = inv ? g.G[1] : g.N[1];
     a.out_q0 = inv ? q0 : 0;
@@ -671,7 +796,7 @@ ColArgs z_pass(const FftGeom &g, bool inv)
     a.nouter = g.G[1];
     a.outer_q0 = 0;
     a.outer_G = g.G[1];
-    const int q0 = wrapi(-(g.N[2] / 2), g.G[2]);
+    const int q0 = wrapi(g.off[2], g.G[2]);
     a.in_q0 = inv ? 0 : q0;
     a.in_n = inv ? g.G[2] : g.N[2];
     a.out_q0 = inv ? q0 : 0;
@@ -714,6 +839,46 @@ int fft3_adjoint(const dmr_plan *p, float2 *grid, int64_t batch, float2 *image, 
     DMR_TRY(launch_cols(g.G[2], g, z_pass(g, true), tw[2], grid, st));
     DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], grid, st));
     return launch_rows(g.G[0], true, g, tw[0], grid, 0, image, st);
+}
+
+bool toep3_applies(int ndim, const int32_t *kshape, const int32_t *ishape)
+{
+    if (fft_disabled() || ndim != 3 || !kshape || !ishape) return false;
+    for (int a = 0; a < 3; a++)
+        if (kshape[a] < ishape[a] || !has_len(kshape[a])) return false;
+    return true;
+}
+
+// Toeplitz self-adjoint of a 3D image batch (src/deepmr/fft/nufft.py:609-669,
+// _interp/toeplitz.py:84-87): zero-pad to the kernel grid (resize offsets
+// K/2 - N/2, no shift), FFT, times kernel[b mod nk] / K (the two orthonormal
+// 1/sqrt(K)), inverse FFT, crop; `data` is a workspace of batch kernel grids.
+int fft3_toeplitz(const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
+                  const void *image, int image_real, float2 *out, int64_t batch, float2 *data, cudaStream_t st)
+{
+    FftGeom g;
+    g.gsize = g.isize = 1;
+    for (int a = 0; a < 3; a++) {
+        g.G[a] = kshape_zyx[2 - a];
+        g.N[a] = ishape_zyx[2 - a];
+        g.off[a] = g.G[a] / 2 - g.N[a] / 2;
+        g.apod[a] = nullptr;
+        g.gsize *= g.G[a];
+        g.isize *= g.N[a];
+    }
+    g.nbf = batch;
+    g.scale = 1.0f;
+    const float2 *tw[3];
+    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    if (batch == 0) return DMR_OK;
+    DMR_TRY(launch_rows(g.G[0], false, g, tw[0], image, image_real, data, st));
+    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, false), tw[1], data, st));
+    ColArgs z = z_pass(g, false);
+    z.out_q0 = z.in_q0;
+    z.out_n = z.in_n;  // only the kept z leave the fused transform
+    DMR_TRY(launch_toep_z(g.G[2], g, z, nk, kernel, (float)(1.0 / (double)g.gsize), tw[2], data, st));
+    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], data, st));
+    return launch_rows(g.G[0], true, g, tw[0], data, 0, out, st);
 }
 
 }  // namespace dmr
