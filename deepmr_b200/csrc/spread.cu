@@ -350,8 +350,11 @@ struct CubeShape {
     static constexpr int NG = NGR <= 1 ? 1 : (NGR <= 2 ? 2 : (NGR <= 4 ? 4 : (NGR <= 8 ? 8 : 16)));
     static constexpr int CUBE = SPL * INS;                                // complex registers
     static constexpr int NW = NDIM * W;                                   // staged weights
+    // staging stride of a sample's weights: odd, so that the two samples a warp
+    // reads at once (16 apart) fall on different banks
+    static constexpr int NWP = NW | 1;
     static constexpr int SB = 128;                                        // staged samples (128: 24.3 vs 26.5 ms 3D gridding, 192^3 kooshball)
-    static size_t meta_bytes() { return (size_t)SB * (NW * sizeof(float) + 2 * sizeof(int)); }
+    static size_t meta_bytes() { return (size_t)SB * (NWP * sizeof(float) + 2 * sizeof(int)); }
 };
 
 // shared-memory geometry of the staged tile + halo for one coil chunk
@@ -382,7 +385,7 @@ __device__ __forceinline__ void stage_cube_samples(const Geom &g, const int org[
                                                    const int32_t *__restrict__ sidx, float *wts,
                                                    int *off, int *gi)
 {
-    constexpr int NW = NDIM * W;
+    constexpr int NW = (NDIM * W) | 1;  // staging stride (CubeShape::NWP)
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         const int j = base + t;
         const float k[3] = {sc0[j], NDIM > 1 ? sc1[j] : 0.0f, NDIM > 2 ? sc2[j] : 0.0f};
@@ -531,7 +534,7 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
     tile_origin(g, it.bin - f * g.nbins, org);
     float2 *tile = reinterpret_cast<float2 *>(smem);
     float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
-    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *off = reinterpret_cast<int *>(wts + S::SB * S::NWP);
     int *gi = off + S::SB;
     const int64_t b0 = (int64_t)blockIdx.y * CC;
     // tile copies in flight while the first batch of weights is computed
@@ -563,7 +566,7 @@ __global__ void __launch_bounds__(kCubeThreads) interp_cube_kernel(
                         for (int j = 0; j < INS; j++) cube[sl][j] = ctile[o + sl * rg.SP + inner_off<NDIM, W>(j, rg.R0)];
                     }
             }
-            const float *w = wts + q * NW;
+            const float *w = wts + q * S::NWP;
             float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
             for (int sl = 0; sl < SPL; sl++) {
@@ -619,7 +622,7 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
     tile_origin(g, it.bin - f * g.nbins, org);
     float2 *tile = reinterpret_cast<float2 *>(smem);
     float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
-    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *off = reinterpret_cast<int *>(wts + S::SB * S::NWP);
     int *gi = off + S::SB;
     for (int e = threadIdx.x; e < CC * rg.PP; e += blockDim.x) tile[e] = make_float2(0.0f, 0.0f);
     const int64_t b0 = (int64_t)blockIdx.y * CC;
@@ -691,7 +694,7 @@ __global__ void __launch_bounds__(kCubeThreads) grid_cube_kernel(
                 pw[k] = pw[k + 1];
             }
             fetch(q + kPf, pv[kPf - 1], pw[kPf - 1]);
-            const float *w = wts + q * NW;
+            const float *w = wts + q * S::NWP;
 #pragma unroll
             for (int sl = 0; sl < SPL; sl++) {
                 if (z0 + sl >= W) continue;
@@ -751,7 +754,7 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
     tile_origin(g, it.bin - f * g.nbins, org);
     float2 *tile = reinterpret_cast<float2 *>(smem);
     float *wts = reinterpret_cast<float *>(tile + (size_t)CC * rg.PP);
-    int *off = reinterpret_cast<int *>(wts + S::SB * NW);
+    int *off = reinterpret_cast<int *>(wts + S::SB * S::NWP);
     int *gi = off + S::SB;
     for (int e = threadIdx.x; e < CC * rg.PP; e += blockDim.x) tile[e] = make_float2(0.0f, 0.0f);
     const int64_t b0 = (int64_t)blockIdx.y * CC;
@@ -803,7 +806,7 @@ __global__ void __launch_bounds__(32 * W) grid_slab_kernel(
             const int64_t o2 = b * g.total + gi[q];
             float2 v = load_sample(ksp, kreal, o2);
             if (weight) v = __fmul2_rn(v, f2(weight[wpb ? o2 : (int64_t)gi[q]]));
-            const float *w = wts + q * NW;
+            const float *w = wts + q * S::NWP;
             const float2 u = __fmul2_rn(f2(w[(NDIM - 1) * W + dz]), v);
 #pragma unroll
             for (int k = 0; k < RL; k++) {
