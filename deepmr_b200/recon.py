@@ -282,6 +282,9 @@ class _Slot:
     def __init__(self, normal, dev, use_graph=True):
         self.stream = torch.cuda.Stream(dev)
         ishape = tuple(normal.ishape)
+        # the result's landing buffer in pinned host memory, allocated once
+        # (a pinned allocation while solves run can synchronise the device)
+        self.host_out = torch.empty(ishape, dtype=torch.complex64, pin_memory=True)
         with torch.cuda.stream(self.stream):
             self.cg = CGState(torch.zeros(ishape, dtype=torch.complex64, device=dev), normal)
             # one eager iteration: cuFFT plans and every lazy setup exist before capture
@@ -452,10 +455,8 @@ class ReconServer:
                 for _ in range(req.niter):
                     a.slot.step()
                 with torch.cuda.stream(a.slot.stream):
-                    # the result leaves the slot (reused) for pinned host memory
-                    x = a.slot.cg.x
-                    a.result = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
-                    a.result.copy_(x, non_blocking=True)
+                    # the result leaves the slot for its pinned host buffer
+                    a.slot.host_out.copy_(a.slot.cg.x, non_blocking=True)
                 a.done_event = torch.cuda.Event()
                 a.done_event.record(a.slot.stream)
                 active.append(a)
@@ -469,8 +470,9 @@ class ReconServer:
                     if a.req.cancelled:
                         stats.errors[a.req.rid] = "cancelled"
                     else:
+                        # a host copy: the slot's buffer is reused by its next request
+                        stats.results[a.req.rid] = a.slot.host_out.clone()
                         stats.latency[a.req.rid] = time.perf_counter() - t0 - a.req.arrival
-                        stats.results[a.req.rid] = a.result
                     self.slots[self._key(a.req)].append(a.slot)
                     used -= a.nbytes
                 else:
