@@ -86,6 +86,43 @@ __device__ __forceinline__ void small_dft(float2 *v, const float2 *tw, bool inv)
         v[0] = make_float2(v[0].x + a.x, v[0].y + a.y);
         v[1] = make_float2(m.x + ib.x, m.y + ib.y);
         v[2] = make_float2(m.x - ib.x, m.y - ib.y);
+    } else if constexpr (R == 7) {
+        // odd R: w^(R-j) = conj(w^j); a_k = v_k + v_(R-k), b_k = v_k - v_(R-k):
+        // V_m, V_(R-m) = v0 + sum_k Re(w^(k m)) a_k +- i sum_k Im(w^(k m)) b_k
+        constexpr int H = R / 2;
+        float2 w[H + 1];
+#pragma unroll
+        for (int j = 1; j <= H; j++) {
+            w[j] = tw[j * (L / R)];
+            if (inv) w[j].y = -w[j].y;
+        }
+        float2 a[H + 1], b[H + 1];
+#pragma unroll
+        for (int k = 1; k <= H; k++) {
+            a[k] = cadd(v[k], v[R - k]);
+            b[k] = csub(v[k], v[R - k]);
+        }
+        float2 o[R];
+        o[0] = v[0];
+#pragma unroll
+        for (int k = 1; k <= H; k++) o[0] = cadd(o[0], a[k]);
+#pragma unroll
+        for (int m = 1; m <= H; m++) {
+            float2 re = v[0], im = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int k = 1; k <= H; k++) {
+                const int j = (k * m) % R;
+                const float c = j <= H ? w[j].x : w[R - j].x;
+                const float sn = j <= H ? w[j].y : -w[R - j].y;
+                re = make_float2(re.x + c * a[k].x, re.y + c * a[k].y);
+                im = make_float2(im.x + sn * b[k].x, im.y + sn * b[k].y);
+            }
+            // i * im = (-im.y, im.x)
+            o[m] = make_float2(re.x - im.y, re.y + im.x);
+            o[R - m] = make_float2(re.x + im.y, re.y - im.x);
+        }
+#pragma unroll
+        for (int m = 0; m < R; m++) v[m] = o[m];
     } else {
         static_assert(R == 5, "radix");
         // w^4 = conj(w), w^3 = conj(w^2); a1 = v1 + v4, b1 = v1 - v4,
@@ -115,7 +152,7 @@ __device__ __forceinline__ void small_dft(float2 *v, const float2 *tw, bool inv)
 
 template <int M>
 struct Split {
-    static constexpr int A = M % 4 == 0 ? 4 : (M % 2 == 0 ? 2 : (M % 3 == 0 ? 3 : 5));
+    static constexpr int A = M % 4 == 0 ? 4 : (M % 2 == 0 ? 2 : (M % 3 == 0 ? 3 : (M % 5 == 0 ? 5 : 7)));
     static constexpr int B = M / A;
 };
 
@@ -126,7 +163,7 @@ struct Split {
 template <int M, int L>
 __device__ __forceinline__ void reg_dft(float2 *v, const float2 *tw, bool inv)
 {
-    if constexpr (M == 2 || M == 3 || M == 4 || M == 5) {
+    if constexpr (M == 2 || M == 3 || M == 4 || M == 5 || M == 7) {
         small_dft<M, L>(v, tw, inv);
     } else {
         constexpr int A = Split<M>::A, B = Split<M>::B;
@@ -159,7 +196,7 @@ __device__ __forceinline__ void reg_dft(float2 *v, const float2 *tw, bool inv)
     }
 }
 
-// A transform length L = L1 L2 (both at most 24, products of 2, 3, 4, 5).
+// A transform length L = L1 L2 (both at most 24, products of 2, 3, 4, 5, 7).
 template <int L_, int L1_, int L2_>
 struct Len {
     static constexpr int L = L_, L1 = L1_, L2 = L2_;
@@ -223,9 +260,11 @@ __device__ __forceinline__ void step_b(const float2 *buf, const float2 *tw, bool
 // the lengths with a compiled transform (grid extents of common matrix sizes
 // at oversampling 1.25 and 2), as (L, L1, L2); other lengths use cuFFT
 #define DMR_FFT_LENGTHS(X)                                                                            \
-    X(32, 8, 4) X(40, 8, 5) X(48, 16, 3) X(64, 8, 8) X(80, 16, 5) X(96, 16, 6) X(120, 12, 10)           \
-    X(128, 16, 8) X(144, 12, 12) X(160, 16, 10) X(192, 16, 12) X(200, 20, 10) X(240, 16, 15)            \
-    X(256, 16, 16) X(288, 18, 16) X(320, 20, 16) X(384, 24, 16) X(400, 20, 20) X(480, 24, 20)
+    X(32, 8, 4) X(40, 8, 5) X(48, 16, 3) X(56, 8, 7) X(64, 8, 8) X(80, 16, 5) X(96, 16, 6)              \
+    X(112, 16, 7) X(120, 12, 10) X(128, 16, 8) X(140, 20, 7) X(144, 12, 12) X(160, 16, 10)               \
+    X(168, 12, 14) X(192, 16, 12) X(200, 20, 10) X(224, 16, 14) X(240, 16, 15) X(256, 16, 16)            \
+    X(280, 20, 14) X(288, 18, 16) X(320, 20, 16) X(336, 24, 14) X(384, 24, 16) X(400, 20, 20)            \
+    X(480, 24, 20)
 
 bool has_len(int L)
 {
@@ -810,8 +849,8 @@ ColArgs z_pass(const FftGeom &g, bool inv)
 bool fft3_applies(const dmr_plan *p)
 {
     const Geom &g = p->g;
-    if (fft_disabled() || g.ndim != 3) return false;
-    for (int a = 0; a < 3; a++)
+    if (fft_disabled() || (g.ndim != 2 && g.ndim != 3)) return false;
+    for (int a = 0; a < g.ndim; a++)
         if (g.G[a] < g.N[a] || !has_len(g.G[a])) return false;
     return true;
 }
@@ -821,11 +860,12 @@ int fft3_forward(const dmr_plan *p, const void *image, int image_real, int64_t b
                  cudaStream_t st)
 {
     const FftGeom g = make_geom(p, batch, 1.0f);
-    const float2 *tw[3];
-    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    const float2 *tw[3] = {nullptr, nullptr, nullptr};
+    for (int a = 0; a < p->g.ndim; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
     if (g.nbf == 0) return DMR_OK;
     DMR_TRY(launch_rows(g.G[0], false, g, tw[0], image, image_real, grid, st));
     DMR_TRY(launch_cols(g.G[1], g, y_pass(g, false), tw[1], grid, st));
+    if (g.G[2] == 1) return DMR_OK;  // 2D
     return launch_cols(g.G[2], g, z_pass(g, false), tw[2], grid, st);
 }
 
@@ -833,18 +873,18 @@ int fft3_forward(const dmr_plan *p, const void *image, int image_real, int64_t b
 int fft3_adjoint(const dmr_plan *p, float2 *grid, int64_t batch, float2 *image, cudaStream_t st)
 {
     const FftGeom g = make_geom(p, batch, (float)(1.0 / (double)p->g.gsize));
-    const float2 *tw[3];
-    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    const float2 *tw[3] = {nullptr, nullptr, nullptr};
+    for (int a = 0; a < p->g.ndim; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
     if (g.nbf == 0) return DMR_OK;
-    DMR_TRY(launch_cols(g.G[2], g, z_pass(g, true), tw[2], grid, st));
+    if (g.G[2] > 1) DMR_TRY(launch_cols(g.G[2], g, z_pass(g, true), tw[2], grid, st));
     DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], grid, st));
     return launch_rows(g.G[0], true, g, tw[0], grid, 0, image, st);
 }
 
 bool toep3_applies(int ndim, const int32_t *kshape, const int32_t *ishape)
 {
-    if (fft_disabled() || ndim != 3 || !kshape || !ishape) return false;
-    for (int a = 0; a < 3; a++)
+    if (fft_disabled() || (ndim != 2 && ndim != 3) || !kshape || !ishape) return false;
+    for (int a = 0; a < ndim; a++)
         if (kshape[a] < ishape[a] || !has_len(kshape[a])) return false;
     return true;
 }
@@ -853,14 +893,14 @@ bool toep3_applies(int ndim, const int32_t *kshape, const int32_t *ishape)
 // _interp/toeplitz.py:84-87): zero-pad to the kernel grid (resize offsets
 // K/2 - N/2, no shift), FFT, times kernel[b mod nk] / K (the two orthonormal
 // 1/sqrt(K)), inverse FFT, crop; `data` is a workspace of batch kernel grids.
-int fft3_toeplitz(const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
+int fft3_toeplitz(int ndim, const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
                   const void *image, int image_real, float2 *out, int64_t batch, float2 *data, cudaStream_t st)
 {
     FftGeom g;
     g.gsize = g.isize = 1;
     for (int a = 0; a < 3; a++) {
-        g.G[a] = kshape_zyx[2 - a];
-        g.N[a] = ishape_zyx[2 - a];
+        g.G[a] = a < ndim ? kshape_zyx[ndim - 1 - a] : 1;
+        g.N[a] = a < ndim ? ishape_zyx[ndim - 1 - a] : 1;
         g.off[a] = g.G[a] / 2 - g.N[a] / 2;
         g.apod[a] = nullptr;
         g.gsize *= g.G[a];
@@ -868,16 +908,25 @@ int fft3_toeplitz(const int32_t *kshape_zyx, const int32_t *ishape_zyx, const fl
     }
     g.nbf = batch;
     g.scale = 1.0f;
-    const float2 *tw[3];
-    for (int a = 0; a < 3; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
+    const float2 *tw[3] = {nullptr, nullptr, nullptr};
+    for (int a = 0; a < ndim; a++) DMR_TRY(twiddles(g.G[a], &tw[a]));
     if (batch == 0) return DMR_OK;
+    const float kscale = (float)(1.0 / (double)g.gsize);
     DMR_TRY(launch_rows(g.G[0], false, g, tw[0], image, image_real, data, st));
-    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, false), tw[1], data, st));
-    ColArgs z = z_pass(g, false);
-    z.out_q0 = z.in_q0;
-    z.out_n = z.in_n;  // only the kept z leave the fused transform
-    DMR_TRY(launch_toep_z(g.G[2], g, z, nk, kernel, (float)(1.0 / (double)g.gsize), tw[2], data, st));
-    DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], data, st));
+    if (ndim == 2) {
+        // the y pass is the fused one: its lines with data in, kept lines out
+        ColArgs y = y_pass(g, false);
+        y.out_q0 = y.in_q0;
+        y.out_n = y.in_n;
+        DMR_TRY(launch_toep_z(g.G[1], g, y, nk, kernel, kscale, tw[1], data, st));
+    } else {
+        DMR_TRY(launch_cols(g.G[1], g, y_pass(g, false), tw[1], data, st));
+        ColArgs z = z_pass(g, false);
+        z.out_q0 = z.in_q0;
+        z.out_n = z.in_n;  // only the kept z leave the fused transform
+        DMR_TRY(launch_toep_z(g.G[2], g, z, nk, kernel, kscale, tw[2], data, st));
+        DMR_TRY(launch_cols(g.G[1], g, y_pass(g, true), tw[1], data, st));
+    }
     return launch_rows(g.G[0], true, g, tw[0], data, 0, out, st);
 }
 

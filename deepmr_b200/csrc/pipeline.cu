@@ -726,8 +726,8 @@ extern "C" int dmr_toeplitz_apply(int ndim, const int32_t *kshape, const int32_t
     std::shared_ptr<FftPlan> fp;
     DMR_TRY(toep_ws(ndim, kshape, batch, workspace, workspace_bytes, &data, &work, &sums, &counts, fp));
     if (toep3_applies(ndim, kshape, ishape))
-        return fft3_toeplitz(kshape, ishape, (const float2 *)kernel, nk, image, image_real, (float2 *)out, batch,
-                             data, st);
+        return fft3_toeplitz(ndim, kshape, ishape, (const float2 *)kernel, nk, image, image_real, (float2 *)out,
+                             batch, data, st);
     ResizeArgs r;
     memset(&r, 0, sizeof(r));
     int64_t ksize = 1, isize = 1;

@@ -93,7 +93,7 @@ int fft3_adjoint(const ::dmr_plan *p, float2 *grid, int64_t batch, float2 *image
 // (kernel extents at least the image's and with a compiled transform), and
 // pad + FFT + kernel multiply + inverse FFT + crop (data: batch kernel grids)
 bool toep3_applies(int ndim, const int32_t *kshape, const int32_t *ishape);
-int fft3_toeplitz(const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
+int fft3_toeplitz(int ndim, const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
                   const void *image, int image_real, float2 *out, int64_t batch, float2 *data, cudaStream_t st);
 // tensor-core atomic gridding of 3D plans (tcgrid.cu); DMR_ERR_UNSUPPORTED when
 // the bin region does not fit

@@ -119,3 +119,57 @@ def test_fused_toeplitz_selfadjoint_vs_oracle(frames):
     out = F.apply_nufft_selfadj(img.cuda(), T)
     assert tuple(out.shape) == tuple(img.shape)
     assert rel(out, R.apply_selfadj(img, To)) < TOL
+
+
+def _coord2(shape, nviews, nsamples, seed, nframes=None):
+    rng = np.random.default_rng(seed)
+    n = np.asarray(shape[::-1], dtype=np.float32)  # (x, y) extents
+    lead = (nviews, nsamples) if nframes is None else (nframes, nviews, nsamples)
+    return (rng.uniform(-0.5, 0.5, lead + (2,)) * n).astype(np.float32)
+
+
+# 2D image shape and oversampling (y, x) -> grid extents with compiled transforms,
+# including a factor 7 (56, 140, 280)
+CASES_2D = [
+    ((20, 24), 2.0, None),            # grid (40, 48)
+    ((45, 37), (1.24, 1.5), None),    # odd extents, grid (56, 56)
+    ((224, 112), 1.25, None),         # grid (280, 140)
+    ((28, 40), 2.0, 3),               # grid (56, 80), 3 frames
+]
+
+
+@pytest.mark.parametrize("shape,os,frames", CASES_2D)
+def test_fused_fft_2d_nufft_vs_oracle(shape, os, frames):
+    import deepmr_b200.fft as F
+    from deepmr_b200 import _lib, synth
+    from oracle import nufft_ref as R
+
+    coord = _coord2(shape, 40, 32, seed=sum(shape), nframes=frames)
+    c = torch.as_tensor(coord)
+    plan = F.plan_nufft(c, shape, 4, os, device="cuda")
+    assert _lib.lib().dmr_fft3_fused(plan.interpolator.handle) == 1
+    oplan = R.plan_nufft(c, shape, 4, os)
+    lead = (4,) + ((frames,) if frames else ())
+    img = synth.complex_gaussian(lead + tuple(shape), seed=1)
+    ksp = synth.complex_gaussian(lead + tuple(c.shape[-3:-1]), seed=2)
+    assert rel(F.apply_nufft(img.cuda(), plan), R.apply_nufft(img, oplan)) < TOL
+    assert rel(F.apply_nufft_adj(ksp.cuda(), plan), R.apply_nufft_adj(ksp, oplan)) < TOL
+
+
+@pytest.mark.parametrize("shape", [(16, 20), (28, 70)])
+def test_fused_toeplitz_2d_vs_oracle(shape):
+    """2D Toeplitz self-adjoint through the fused passes (kernel grids 2N with
+    compiled transforms, one with a factor 7): the y pass is the fused
+    forward FFT, kernel multiply and inverse FFT."""
+    import deepmr_b200.fft as F
+    from oracle import nufft_ref as R
+
+    coord = _coord2(shape, 30, 40, seed=21)
+    c = torch.as_tensor(coord)
+    dcf = torch.rand(tuple(c.shape[:-1]), generator=torch.Generator().manual_seed(22)) + 0.5
+    T = F.plan_toeplitz_nufft(c, shape, dcf=dcf, device="cuda")
+    To = R.plan_toeplitz(c, shape, dcf=dcf)
+    g = torch.Generator().manual_seed(23)
+    img = torch.complex(torch.randn((5,) + shape, generator=g), torch.randn((5,) + shape, generator=g))
+    out = F.apply_nufft_selfadj(img.cuda(), T)
+    assert rel(out, R.apply_selfadj(img, To)) < TOL
