@@ -95,8 +95,8 @@ int fft3_adjoint(const ::dmr_plan *p, float2 *grid, int64_t batch, float2 *image
 bool toep3_applies(int ndim, const int32_t *kshape, const int32_t *ishape);
 int fft3_toeplitz(int ndim, const int32_t *kshape_zyx, const int32_t *ishape_zyx, const float2 *kernel, int64_t nk,
                   const void *image, int image_real, float2 *out, int64_t batch, float2 *data, cudaStream_t st);
-// tensor-core atomic gridding of 3D plans (tcgrid.cu); DMR_ERR_UNSUPPORTED when
-// the bin region does not fit
+// tensor-core gridding of 3D plans (tcgrid.cu: dispatch and health state,
+// tmgrid.cu: the kernel); DMR_ERR_UNSUPPORTED when the plan has no gridding bins
 int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
                      cudaStream_t st);

@@ -445,6 +445,12 @@ def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
 # separate copy engines), instead of copy in -> compute -> copy out in series.
 PIPELINE_MIN_BYTES = 64 << 20
 PIPELINE_CHUNKS = 8
+# batch items per chunk of a host-pipelined 3D adjoint, at least: atomic
+# gridding of a few coils runs on the CUDA cores at a cost proportional to the
+# coils; the deterministic tensor-core gridding costs about the same for 8
+# coils as for 32
+ADJOINT_MIN_CHUNK_3D = 4
+ADJOINT_MIN_CHUNK_3D_DET = 8
 
 _PIPE_STREAMS = {}
 
@@ -612,11 +618,7 @@ def _apply_nufft_adj(kspace, nufft_plan, basis, weight, device, threadsperblock,
             )
         )
 
-    # chunks of a 3D adjoint: atomic gridding of a few coils runs on the CUDA
-    # cores at a cost proportional to the coils, so 4 per chunk; the
-    # deterministic tensor-core gridding costs about the same for 8 coils as
-    # for 32, so at least 8
-    min_chunk = (8 if det else 4) if nufft_plan.ndim == 3 else 1
+    min_chunk = (ADJOINT_MIN_CHUNK_3D_DET if det else ADJOINT_MIN_CHUNK_3D) if nufft_plan.ndim == 3 else 1
     if batch >= 2 * min_chunk and _pipelinable(kspace, dev, batch, 8 * int(np.prod(item))):
         w, wpb = _weight_arg(weight, batch_shape, interp, frames_shape, dev)
         out = torch.empty([batch] + item, dtype=torch.complex64, pin_memory=True)
