@@ -444,12 +444,12 @@ def _weight_arg(weight, batch_shape, interp, frames_shape, dev):
 # previous chunk and the copy out of the one before overlap (H2D and D2H run on
 # separate copy engines), instead of copy in -> compute -> copy out in series.
 PIPELINE_MIN_BYTES = 64 << 20
-PIPELINE_CHUNKS = 8
+PIPELINE_CHUNKS = 16
 # batch items per chunk of a host-pipelined 3D adjoint, at least: atomic
 # gridding of a few coils runs on the CUDA cores at a cost proportional to the
 # coils; the deterministic tensor-core gridding costs about the same for 8
 # coils as for 32
-ADJOINT_MIN_CHUNK_3D = 4
+ADJOINT_MIN_CHUNK_3D = 2
 ADJOINT_MIN_CHUNK_3D_DET = 8
 
 _PIPE_STREAMS = {}
