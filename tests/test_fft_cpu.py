@@ -22,12 +22,13 @@ def test_centred_fft_matches_numpy_and_round_trips():
     np.testing.assert_allclose(t.numpy(), np.fft.fft(x, axis=1), rtol=1e-4, atol=1e-4)
 
 
-@pytest.mark.parametrize("batch,min_chunk,expect", [(32, 1, (8, 4)), (32, 8, (4, 8)), (5, 1, (5, 1)),
-                                                     (11, 1, (6, 2)), (16, 8, (2, 8)), (12, 8, (1, 12)),
-                                                     (1, 1, (1, 1))])
+@pytest.mark.parametrize("batch,min_chunk,expect", [(32, 1, (16, 2)), (32, 2, (16, 2)), (32, 8, (4, 8)),
+                                                     (5, 1, (5, 1)), (40, 1, (14, 3)), (16, 8, (2, 8)),
+                                                     (12, 8, (1, 12)), (1, 1, (1, 1))])
 def test_host_pipeline_chunks(batch, min_chunk, expect):
-    """Chunking of the pinned-host pipeline: at most 8 chunks, at least
-    min_chunk items each (3D adjoints use 8), the last one possibly shorter."""
+    """Chunking of the pinned-host pipeline: at most 16 chunks, at least
+    min_chunk items each (3D adjoints use 2, deterministic ones 8), the last
+    one possibly shorter."""
     import importlib
 
     N = importlib.import_module("deepmr_b200.fft.nufft")
