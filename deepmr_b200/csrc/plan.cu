@@ -160,26 +160,6 @@ __global__ void tg_weights_kernel(Geom g, int t0, int t1, int t2, int wp, const 
     }
 }
 
-// Smallest colour period C along one axis such that bins b1 != b2 with
-// b1 = b2 (mod C) have disjoint regions [b T, b T + ext) (mod G).
-static int axis_colours(int nb, int T, int G, int ext)
-{
-    int C = std::max(1, (int)ceil_div(ext, T));
-    for (; C < nb; C++) {
-        bool ok = true;
-        for (int b1 = 0; b1 < nb && ok; b1++)
-            for (int b2 = b1 + 1; b2 < nb && ok; b2++) {
-                if (b1 % C != b2 % C) continue;
-                for (int i = 0; i < ext && ok; i++) {
-                    const int x = (b1 * T + i) % G;
-                    if (pmod(x - b2 * T, G) < ext) ok = false;
-                }
-            }
-        if (ok) break;
-    }
-    return std::min(C, nb);
-}
-
 // Work items of at most `chunk` samples per non-empty bin, and their visiting
 // order in 4 x 4 x 4-bin tiles (frame, tile z, y, x, bin z, y, x), so that
 // bins sharing halo points or spokes run close together.
@@ -543,65 +523,15 @@ extern "C" int dmr_plan_create(int ndim, const int32_t *shape, const int32_t *os
                 DMR_CUDA(cudaMemcpyAsync(p->tg_order, torder.data(), torder.size() * sizeof(int32_t),
                                          cudaMemcpyHostToDevice, st));
             }
-            // deterministic mode: whole bins by colour, heaviest first
-            int C[3];
-            for (int a = 0; a < 3; a++) C[a] = axis_colours(tnb[a], tT[a], g.G[a], tT[a] + W - 1);
-            const int ncol = C[0] * C[1] * C[2];
-            std::vector<std::vector<WorkItem>> byc(ncol);
-            for (int64_t key = 0; key < tkeys; key++) {
-                if (ts[key + 1] == ts[key]) continue;
-                const int lb = (int)(key % tbins);
-                const int bx = lb % tnb[0], by = (lb / tnb[0]) % tnb[1], bz = lb / (tnb[0] * tnb[1]);
-                byc[(bz % C[2] * C[1] + by % C[1]) * C[0] + bx % C[0]].push_back({(int)key, ts[key], ts[key + 1]});
-            }
-            // heavy bins are split into segments of kTgSegment samples with a
-            // scratch slot each (slots numbered per colour: the colours run in
-            // order and reuse the scratch)
-            std::vector<WorkItem> det, red;
-            std::vector<int32_t> dslot;
-            p->tg_det_cstart.assign(1, 0);
-            p->tg_det_rstart.assign(1, 0);
-            p->tg_det_slots = 0;
-            for (int c = 0; c < ncol; c++) {
-                std::stable_sort(byc[c].begin(), byc[c].end(), [](const WorkItem &x, const WorkItem &y) {
-                    return (x.end - x.begin) > (y.end - y.begin);
-                });
-                int ns = 0;
-                for (const WorkItem &w : byc[c]) {
-                    if (w.end - w.begin <= kTgSegment) {
-                        det.push_back(w);
-                        dslot.push_back(-1);
-                        continue;
-                    }
-                    const int s0 = ns;
-                    for (int s = w.begin; s < w.end; s += kTgSegment) {
-                        det.push_back({w.bin, s, std::min(s + kTgSegment, w.end)});
-                        dslot.push_back(ns++);
-                    }
-                    red.push_back({w.bin, s0, ns});
-                }
-                p->tg_det_slots = std::max(p->tg_det_slots, ns);
-                p->tg_det_cstart.push_back((int)det.size());
-                p->tg_det_rstart.push_back((int)red.size());
-            }
-            std::vector<int32_t> iota(std::max(det.size(), titems.size()));
-            for (size_t i = 0; i < iota.size(); i++) iota[i] = (int32_t)i;
-            DMR_TRY(dev_alloc(&p->tg_det_work, det.size()));
-            DMR_TRY(dev_alloc(&p->tg_det_slot, dslot.size()));
-            DMR_TRY(dev_alloc(&p->tg_det_red, red.size()));
-            DMR_TRY(dev_alloc(&p->tg_iota, iota.size()));
-            if (!det.empty()) {
-                DMR_CUDA(cudaMemcpyAsync(p->tg_det_work, det.data(), det.size() * sizeof(WorkItem),
-                                         cudaMemcpyHostToDevice, st));
-                DMR_CUDA(cudaMemcpyAsync(p->tg_det_slot, dslot.data(), dslot.size() * sizeof(int32_t),
-                                         cudaMemcpyHostToDevice, st));
-            }
-            if (!red.empty())
-                DMR_CUDA(cudaMemcpyAsync(p->tg_det_red, red.data(), red.size() * sizeof(WorkItem),
-                                         cudaMemcpyHostToDevice, st));
-            if (!iota.empty())
-                DMR_CUDA(cudaMemcpyAsync(p->tg_iota, iota.data(), iota.size() * sizeof(int32_t),
-                                         cudaMemcpyHostToDevice, st));
+            // deterministic mode: the items of each bin (make_items numbers
+            // them in key order, kTgSegment samples each)
+            std::vector<int32_t> istart(tkeys + 1, 0);
+            for (int64_t k = 0; k < tkeys; k++)
+                istart[k + 1] = istart[k] + (int32_t)ceil_div(ts[k + 1] - ts[k], kTgSegment);
+            DMR_CHECK(istart[tkeys] == (int64_t)titems.size(), DMR_ERR_UNSUPPORTED, "gridding item count mismatch");
+            DMR_TRY(dev_alloc(&p->tg_item_start, istart.size()));
+            DMR_CUDA(cudaMemcpyAsync(p->tg_item_start, istart.data(), istart.size() * sizeof(int32_t),
+                                     cudaMemcpyHostToDevice, st));
             DMR_CUDA(cudaStreamSynchronize(st));
             p->tg_nwork = (int)titems.size();
             p->tg_nbins = tbins;

@@ -74,7 +74,8 @@ std::shared_ptr<FftPlan> get_fft_plan(int ndim, const int *dims_zyx, int64_t bat
 bool rt_geometry_ok(const Geom &g);
 int rt_build(::dmr_plan *p, const std::vector<int32_t> &h_start, cudaStream_t st);
 size_t rt_scratch_bytes(const ::dmr_plan *p, int64_t batch);
-// scratch bytes of deterministic tensor-core gridding (split bins' partial sums)
+// scratch bytes of deterministic tensor-core gridding (every work item's
+// region partial sums, 2 KB per item and coil)
 size_t tm_scratch_bytes(const ::dmr_plan *p, int64_t batch);
 // scratch bytes a gridding call of `batch` coils may need (either kernel)
 size_t grid_scratch_bytes(const ::dmr_plan *p, int64_t batch);
@@ -101,8 +102,9 @@ int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *gr
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
                      cudaStream_t st);
 // tensor-core gridding with the plan's gridding bins (tmgrid.cu), atomic or
-// deterministic (colour launches; scratch from the caller when it holds
-// tm_scratch_bytes, else from the library pool); `timeouts` is the device
+// deterministic (partial sums per work item, then a gather per grid point;
+// scratch from the caller when it holds tm_scratch_bytes, else from the
+// library pool); `timeouts` is the device
 // address of the process-wide counter of blocks that stopped on a bounded wait
 int grid_tm_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes, int *timeouts,
@@ -139,20 +141,10 @@ struct dmr_plan {
     dmr::WorkItem *tg_work = nullptr;
     int tg_nwork = 0;
     int32_t *tg_order = nullptr;
-    // deterministic mode: bins grouped by colour (bins of one colour have
-    // disjoint regions; colours run in order), heaviest first within a colour.
-    // A bin of more than dmr::kTgSegment samples is split into segments of that
-    // many, which run in parallel and write partial sums to scratch slot
-    // tg_det_slot[item] (-1: the item adds into the grid, the only addition to
-    // its points in the colour); the colour's reduction items (bin, first slot,
-    // end slot) then add the slots of each split bin in slot order.
-    dmr::WorkItem *tg_det_work = nullptr;
-    int32_t *tg_det_slot = nullptr;
-    dmr::WorkItem *tg_det_red = nullptr;
-    int32_t *tg_iota = nullptr;          // 0, 1, 2, ... (identity visiting order)
-    std::vector<int> tg_det_cstart;      // host, ncolours + 1 (items)
-    std::vector<int> tg_det_rstart;      // host, ncolours + 1 (reduction items)
-    int tg_det_slots = 0;                // scratch slots of one colour, at most
+    // deterministic mode: the items of each bin, [tg_item_start[k],
+    // tg_item_start[k + 1]) of tg_work for bin key k (frame * tg_nbins + bin;
+    // items are numbered in key order, a bin's segments in sample order)
+    int32_t *tg_item_start = nullptr;
     int32_t *bin_start = nullptr;       // (nframes * nbins + 1)
     dmr::WorkItem *work = nullptr;      // interpolation / atomic gridding items
     int nwork = 0;
@@ -189,10 +181,7 @@ struct dmr_plan {
         cudaFree(tg_l);
         cudaFree(tg_work);
         cudaFree(tg_order);
-        cudaFree(tg_det_work);
-        cudaFree(tg_det_slot);
-        cudaFree(tg_det_red);
-        cudaFree(tg_iota);
+        cudaFree(tg_item_start);
         cudaFree(bin_start);
         cudaFree(work);
         cudaFree(work_order);

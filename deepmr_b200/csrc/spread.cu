@@ -1394,9 +1394,11 @@ int interp_dispatch(const dmr_plan *p, const float2 *grid, float2 *ksp, int64_t 
 int grid_rt_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, void *scratch, size_t scratch_bytes, cudaStream_t st);
 
+// (the deterministic tensor-core gridding takes its larger scratch from the
+// library pool, so that callers' workspaces do not hold it in atomic mode)
 size_t grid_scratch_bytes(const dmr_plan *p, int64_t batch)
 {
-    return std::max(rt_scratch_bytes(p, batch), tm_scratch_bytes(p, batch));
+    return rt_scratch_bytes(p, batch);
 }
 
 // minimum coil count of atomic tensor-core gridding (dmr_tc_min_coils)
@@ -1406,8 +1408,9 @@ int grid_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, i
                   const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,
                   cudaStream_t st)
 {
-    // 3D gridding on the tensor cores: atomic, or deterministic in colour
-    // launches (bitwise reproducible), when the plan's gridding bins apply.
+    // 3D gridding on the tensor cores: atomic, or deterministic (per-item
+    // partial sums gathered per grid point in a fixed order, bitwise
+    // reproducible), when the plan's gridding bins apply.
     // Its cost is mostly per sample (the spreading operand and the region
     // read-back are built for all 32 coil slots), so atomic gridding of fewer
     // coils runs on the CUDA cores, whose cost scales with the coil count

@@ -47,7 +47,7 @@ static int timeouts_ptr(int dev, int **out)
 }
 
 // Tensor-core gridding of a 3D plan with the kernel of tmgrid.cu (atomic, or
-// deterministic in colour launches); DMR_ERR_UNSUPPORTED when it does not
+// deterministic through per-item partial sums); DMR_ERR_UNSUPPORTED when it does not
 // apply or DMR_NO_TC=1 (then the caller uses the CUDA-core kernels).
 int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes,

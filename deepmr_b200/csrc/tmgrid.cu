@@ -263,8 +263,8 @@ __device__ __forceinline__ void bin_origin(const Geom &g, int bin, int &f, int o
 __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
     Geom g, TmShape sh, const WorkItem *__restrict__ work, const int32_t *__restrict__ order, int nwork,
     int nchunks, const float *__restrict__ tw, const int32_t *__restrict__ tl, const int32_t *__restrict__ sidx, const void *__restrict__ ksp, int kreal, float2 *__restrict__ grid,
-    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale, const int32_t *__restrict__ dslot,
-    float2 *__restrict__ scratch, int *__restrict__ status, int *__restrict__ timeouts, int stall)
+    int64_t batch, const float *__restrict__ weight, int wpb, float inv_scale, float2 *__restrict__ scratch,
+    int *__restrict__ status, int *__restrict__ timeouts, int stall)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[kBarCount];
@@ -492,10 +492,11 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                 goff[et] = (gz * g.G[1] + gy) * g.G[0] + gx;
             }
             const float2 *gitem = grid + (b0 * g.nframes + f) * g.gsize;
-            // a segment of a split bin (deterministic mode) stores its partial
-            // sums into its scratch slot, [coil][region point]
-            const int dsl = dslot ? dslot[order[ps.task / nchunks]] : -1;
-            float2 *part = dsl >= 0 ? scratch + ((int64_t)dsl * nchunks + ps.task % nchunks) * sh.CC * kTmN : nullptr;
+            // deterministic mode: the item stores its partial sums into its
+            // scratch slot (the item's index), [coil][region point]
+            float2 *part = scratch ? scratch + ((int64_t)order[ps.task / nchunks] * nchunks + ps.task % nchunks) *
+                                                   sh.CC * kTmN
+                                   : nullptr;
             const int64_t cstride = (int64_t)g.nframes * g.gsize;
             uint32_t r[16], rn[16];
             tc_ld16(tbase + lanebase + (uint32_t)(acc * kTmN + 16 * hcol), r);
@@ -528,7 +529,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
 #pragma unroll
                         for (int cc = 0; cc < 4; cc++) {
                             const int c = e * 4 + cc;
-                            if (c < cact) part[c * kTmN + pp] = v[cc];
+                            if (c < cact) __stcs(part + c * kTmN + pp, v[cc]);
                         }
                     } else {
 #pragma unroll
@@ -694,40 +695,102 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
     }
 }
 
-// Deterministic mode: the split bins of one colour (reduction items: bin,
-// first slot, end slot) add their segments' partial sums, in slot order, into
-// the grid; one block per (item, coil block), thread = (coil, region point).
-// No other block of the launch touches the bin's region points.
-__global__ void __launch_bounds__(256) grid_tm_reduce_kernel(Geom g, TmShape sh, const WorkItem *__restrict__ red,
-                                                            const float2 *__restrict__ scratch, float2 *grid,
-                                                            int64_t batch, int nchunks)
+// The regions that cover grid position `pos` along one axis: bins b with
+// offsets u in their region, (b T + u - half) = pos (mod G), 0 <= u < R <= 8,
+// as 16-bit entries (b << 3 | u) + 1 in increasing u, 0 after the last. With
+// R <= G a bin covers a position at most once; b T = (pos + half - u) mod G
+// < G implies b < nb. Increasing u puts neighbouring positions of one bin at
+// the same index.
+__device__ __forceinline__ uint4 tm_cover(int pos, int G, int T, int R, int half)
 {
-    const WorkItem r = red[blockIdx.x];
-    const int cch = blockIdx.y;
-    int f, org[3];
-    bin_origin(g, r.bin, f, org);
-    const int64_t b0 = (int64_t)cch * sh.CC;
-    const int cact = (int)(batch - b0 < (int64_t)sh.CC ? batch - b0 : (int64_t)sh.CC);
-    const int RXY = sh.R[0] * sh.R[1];
-    const int64_t sstride = (int64_t)nchunks * sh.CC * kTmN;
-    const float2 *src = scratch + ((int64_t)r.begin * nchunks + cch) * sh.CC * kTmN;
-    for (int e = threadIdx.x; e < cact * kTmN; e += blockDim.x) {
-        const int c = e / kTmN, pt = e - c * kTmN;
-        if (pt >= sh.P) continue;
-        float2 acc = make_float2(0.0f, 0.0f);
-        for (int s = 0; s < r.end - r.begin; s++) {
-            const float2 v = src[s * sstride + e];
-            acc.x += v.x;
-            acc.y += v.y;
+    uint32_t e[4] = {0, 0, 0, 0};
+    int n = 0;
+    const int t = (pos + half) % G;
+    for (int u = 0; u < R; u++) {
+        int o = t - u;
+        if (o < 0) o += G;
+        if (o % T == 0) {
+            e[n >> 1] |= (uint32_t)((o / T) << 3 | u) + 1u << (16 * (n & 1));
+            n++;
         }
-        const int pz = pt / RXY, pr = pt - pz * RXY;
-        const int py = pr / sh.R[0], px = pr - py * sh.R[0];
-        const int gx = (org[0] + px + g.G[0] - g.half[0]) % g.G[0];
-        const int gy = (org[1] + py + g.G[1] - g.half[1]) % g.G[1];
-        const int gz = (org[2] + pz + g.G[2] - g.half[2]) % g.G[2];
-        float2 *gp = grid + ((b0 + c) * g.nframes + f) * g.gsize + (gz * g.G[1] + gy) * g.G[0] + gx;
-        const float2 o = *gp;
-        *gp = make_float2(o.x + acc.x, o.y + acc.y);
+    }
+    return make_uint4(e[0], e[1], e[2], e[3]);
+}
+
+__device__ __forceinline__ int tm_cover_at(const uint4 &c, int k)
+{
+    const int q = k >> 1;  // entries 2q and 2q + 1 share a word
+    const uint32_t w = q < 2 ? (q < 1 ? c.x : c.y) : (q < 3 ? c.z : c.w);
+    return (int)((w >> (16 * (k & 1))) & 0xffff) - 1;
+}
+
+// Deterministic mode: every grid point adds, for kTmGatherCoils coils of one
+// coil chunk (blockIdx.y: chunk, coil group), in a fixed order (covering bins
+// by z, y, x offset, then each bin's items in sample order) the partial sums
+// that the covering items stored in their scratch slots, and writes the grid
+// once (0 where no item covers it). Lanes run along x, so a warp reads groups
+// of neighbouring region points of a few slots and writes 32 neighbouring
+// grid points per coil; the coil groups run one after another over the grid,
+// so the slots that one grid plane reads stay in L2 between its rows. The
+// cover lists of all positions (two entries per 32-bit word, up to 8 per
+// position) are built per block in shared memory (G[0] + G[1] + G[2] uint4).
+constexpr int kTmGatherCoils = 8;
+
+__global__ void __launch_bounds__(256) grid_tm_gather_kernel(Geom g, TmShape sh, const int32_t *__restrict__ istart,
+                                                            const float2 *__restrict__ scratch,
+                                                            float2 *__restrict__ grid, int64_t batch, int nchunks)
+{
+    extern __shared__ uint4 s_cover[];
+    uint4 *cov[3] = {s_cover, s_cover + g.G[0], s_cover + g.G[0] + g.G[1]};
+    for (int a = 0; a < 3; a++)
+        for (int pos = threadIdx.x; pos < g.G[a]; pos += blockDim.x)
+            cov[a][pos] = tm_cover(pos, g.G[a], g.T[a], sh.R[a], g.half[a]);
+    __syncthreads();
+    const int ngrp = (sh.CC + kTmGatherCoils - 1) / kTmGatherCoils;
+    const int cch = blockIdx.y / ngrp, c0 = (blockIdx.y % ngrp) * kTmGatherCoils;
+    const int64_t b0 = (int64_t)cch * sh.CC + c0;
+    // coils of this chunk (the last chunk may hold fewer than CC), of this group
+    const int ccoils = (int)min((int64_t)sh.CC, batch - (int64_t)cch * sh.CC);
+    const int cact = min(kTmGatherCoils, ccoils - c0);
+    const int64_t npts = (int64_t)g.nframes * g.gsize;
+    const int gxy = g.G[0] * g.G[1];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(i / g.gsize), r = (int)(i - (int64_t)f * g.gsize);
+        const int z = r / gxy, y = (r - z * gxy) / g.G[0], x = r - z * gxy - y * g.G[0];
+        const uint4 cz = cov[2][z], cy = cov[1][y], cx = cov[0][x];
+        float2 acc[kTmGatherCoils];
+#pragma unroll
+        for (int c = 0; c < kTmGatherCoils; c++) acc[c] = make_float2(0.0f, 0.0f);
+        for (int kz = 0; kz < 8; kz++) {
+            const int vz = tm_cover_at(cz, kz);
+            if (vz < 0) break;
+            for (int ky = 0; ky < 8; ky++) {
+                const int vy = tm_cover_at(cy, ky);
+                if (vy < 0) break;
+                const int kyz = f * g.nbins + ((vz >> 3) * g.nb[1] + (vy >> 3)) * g.nb[0];
+                const int pyz = ((vz & 7) * sh.R[1] + (vy & 7)) * sh.R[0];
+                for (int kx = 0; kx < 8; kx++) {
+                    const int vx = tm_cover_at(cx, kx);
+                    if (vx < 0) break;
+                    const int key = kyz + (vx >> 3);
+                    const int s1 = istart[key + 1];
+                    const int pt = pyz + (vx & 7);
+                    for (int s = istart[key]; s < s1; s++) {
+                        const float2 *src = scratch + (((int64_t)s * nchunks + cch) * sh.CC + c0) * kTmN + pt;
+#pragma unroll
+                        for (int c = 0; c < kTmGatherCoils; c++)
+                            if (c < cact) {
+                                const float2 v = __ldg(src + c * kTmN);
+                                acc[c].x += v.x;
+                                acc[c].y += v.y;
+                            }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kTmGatherCoils; c++)
+            if (c < cact) grid[(b0 + c) * npts + i] = acc[c];
     }
 }
 
@@ -780,11 +843,13 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
 // Tensor-core gridding of a 3D plan with its gridding bins; DMR_ERR_UNSUPPORTED
 // when the plan has none or the geometry does not fit (the caller then uses
 // the other kernels).
+// scratch of deterministic tensor-core gridding: one slot of kTmN region
+// points per (work item, coil)
 size_t tm_scratch_bytes(const dmr_plan *p, int64_t batch)
 {
-    if (p->g.ndim != 3 || p->tg_T[0] == 0 || p->tg_det_slots == 0 || batch < 1) return 0;
+    if (p->g.ndim != 3 || p->tg_T[0] == 0 || p->tg_nwork == 0 || batch < 1) return 0;
     const int64_t cc = std::min<int64_t>(batch, kTmCC);
-    return (size_t)p->tg_det_slots * ceil_div(batch, cc) * cc * kTmN * sizeof(float2);
+    return (size_t)p->tg_nwork * ceil_div(batch, cc) * cc * kTmN * sizeof(float2);
 }
 
 int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
@@ -805,11 +870,14 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     int per_sm = 0;
     DMR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_tmem_kernel, kTmThreads, smem));
     if (per_sm != 1) return DMR_ERR_UNSUPPORTED;
-    // deterministic mode needs the points of one region on distinct grid points
+    // deterministic mode needs the points of one region on distinct grid
+    // points and at most 8 region points per axis (the gather's cover lists)
     if (det)
         for (int a = 0; a < 3; a++)
-            if (sh.R[a] > p->g.G[a]) return DMR_ERR_UNSUPPORTED;
-    DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
+            if (sh.R[a] > p->g.G[a] || sh.R[a] > 8) return DMR_ERR_UNSUPPORTED;
+    // the deterministic gather writes every grid point
+    if (!det || p->tg_nwork == 0)
+        DMR_CUDA(cudaMemsetAsync(grid, 0, (size_t)batch * p->g.nframes * p->g.gsize * sizeof(float2), st));
     if (p->tg_nwork == 0) return DMR_OK;
     const int64_t nchunks = ceil_div(batch, sh.CC);
     DMR_CHECK((int64_t)p->tg_nwork * nchunks < (1ll << 31), DMR_ERR_UNSUPPORTED, "too many gridding tasks");
@@ -825,45 +893,45 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
         const int blocks = (int)std::min<int64_t>((int64_t)p->tg_nwork * nchunks, (int64_t)sms);
         grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
             g, sh, p->tg_work, p->tg_order, p->tg_nwork, (int)nchunks, p->tg_w, p->tg_l, p->tg_sidx, ksp, kreal,
-            grid, batch, weight, wpb, inv_scale, nullptr, nullptr, p->status, timeouts, stall);
+            grid, batch, weight, wpb, inv_scale, nullptr, p->status, timeouts, stall);
         DMR_LAUNCHED("grid_tmem_kernel");
         return DMR_OK;
     }
-    // deterministic: one launch per colour; within a launch no two bins touch
-    // the same grid point, a whole bin adds into the grid once and a split
-    // bin's segments write scratch slots that the colour's reduction adds in
-    // slot order; the launches run in order on the stream, so every grid point
-    // is summed in the same order in every run
+    // deterministic: the items store their partial sums into scratch slots
+    // (no grid writes), then the gather sums them per grid point in a fixed
+    // order: every run adds the same values in the same order
+    const int ngrp = (sh.CC + kTmGatherCoils - 1) / kTmGatherCoils;
+    DMR_CHECK(nchunks * ngrp <= 65535, DMR_ERR_UNSUPPORTED, "batch too large");
+    // the gather's cover lists: one uint4 per grid position of each axis
+    const size_t gsmem = (size_t)(p->g.G[0] + p->g.G[1] + p->g.G[2]) * sizeof(uint4);
+    if (gsmem > 48 * 1024) {
+        DMR_CHECK(gsmem <= (size_t)smem_blk, DMR_ERR_UNSUPPORTED, "grid too large for the gather");
+        DMR_CUDA(cudaFuncSetAttribute(grid_tm_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
+    }
     const size_t need = tm_scratch_bytes(p, batch);
     void *owned = nullptr;
-    if (need > 0 && (scratch == nullptr || scratch_bytes < need)) {
+    if (scratch == nullptr || scratch_bytes < need) {
         cudaMemPool_t pool = scratch_pool(p->device);
         DMR_CHECK(pool != nullptr, DMR_ERR_CUDA, "no memory pool for the gridding scratch");
         DMR_CUDA(cudaMallocFromPoolAsync(&owned, need, pool, st));
         scratch = owned;
     }
     int rc = DMR_OK;
-    for (size_t c = 0; c + 1 < p->tg_det_cstart.size() && rc == DMR_OK; c++) {
-        const int n = p->tg_det_cstart[c + 1] - p->tg_det_cstart[c];
-        if (n == 0) continue;
-        const int blocks = (int)std::min<int64_t>((int64_t)n * nchunks, (int64_t)sms);
-        grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
-            g, sh, p->tg_det_work + p->tg_det_cstart[c], p->tg_iota, n, (int)nchunks, p->tg_w, p->tg_l,
-            p->tg_sidx, ksp, kreal, grid, batch, weight, wpb, inv_scale, p->tg_det_slot + p->tg_det_cstart[c],
-            (float2 *)scratch, p->status, timeouts, stall);
-        g_launches.fetch_add(1, std::memory_order_relaxed);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            rc = cuda_fail(e, "grid_tmem_kernel", __FILE__, __LINE__);
-            break;
-        }
-        const int nr = p->tg_det_rstart[c + 1] - p->tg_det_rstart[c];
-        if (nr == 0) continue;
-        grid_tm_reduce_kernel<<<dim3(nr, (unsigned)nchunks), 256, 0, st>>>(
-            g, sh, p->tg_det_red + p->tg_det_rstart[c], (const float2 *)scratch, grid, batch, (int)nchunks);
+    const int blocks = (int)std::min<int64_t>((int64_t)p->tg_nwork * nchunks, (int64_t)sms);
+    grid_tmem_kernel<<<blocks, kTmThreads, smem, st>>>(
+        g, sh, p->tg_work, p->tg_order, p->tg_nwork, (int)nchunks, p->tg_w, p->tg_l, p->tg_sidx, ksp, kreal, grid,
+        batch, weight, wpb, inv_scale, (float2 *)scratch, p->status, timeouts, stall);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_fail(e, "grid_tmem_kernel", __FILE__, __LINE__);
+    if (rc == DMR_OK) {
+        const int64_t npts = (int64_t)g.nframes * g.gsize;
+        const int gblocks = (int)std::min<int64_t>(ceil_div(npts, 256), (int64_t)sms * 16);
+        grid_tm_gather_kernel<<<dim3(gblocks, (unsigned)(nchunks * ngrp)), 256, gsmem, st>>>(
+            g, sh, p->tg_item_start, (const float2 *)scratch, grid, batch, (int)nchunks);
         g_launches.fetch_add(1, std::memory_order_relaxed);
         e = cudaGetLastError();
-        if (e != cudaSuccess) rc = cuda_fail(e, "grid_tm_reduce_kernel", __FILE__, __LINE__);
+        if (e != cudaSuccess) rc = cuda_fail(e, "grid_tm_gather_kernel", __FILE__, __LINE__);
     }
     if (owned) cudaFreeAsync(owned, st);
     return rc;
