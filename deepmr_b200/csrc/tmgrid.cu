@@ -107,6 +107,7 @@ struct TmShape {
     int R[3];        // region extents (tile + W - 1)
     int P;           // region points (<= 256)
     int CC;          // coils per block (<= 32)
+    int ccp;         // deterministic scratch: coil stride of a region point (CC rounded up to 8)
     int vrows;       // R[0] + R[1] + R[2]
     int table_off;   // per builder group two chunk weight tables (offset in dynamic shared memory)
     int goff_off;    // read-back: grid offsets of the current item's region points
@@ -493,9 +494,9 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             }
             const float2 *gitem = grid + (b0 * g.nframes + f) * g.gsize;
             // deterministic mode: the item stores its partial sums into its
-            // scratch slot (the item's index), [coil][region point]
+            // scratch slot (the item's index), [region point][coil]
             float2 *part = scratch ? scratch + ((int64_t)order[ps.task / nchunks] * nchunks + ps.task % nchunks) *
-                                                   sh.CC * kTmN
+                                                   kTmN * sh.ccp
                                    : nullptr;
             const int64_t cstride = (int64_t)g.nframes * g.gsize;
             uint32_t r[16], rn[16];
@@ -526,11 +527,15 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                                                 inv_scale);
                     }
                     if (part) {
-#pragma unroll
-                        for (int cc = 0; cc < 4; cc++) {
-                            const int c = e * 4 + cc;
-                            if (c < cact) __stcs(part + c * kTmN + pp, v[cc]);
-                        }
+                        // coils 4e .. 4e + 3 of the point: one 32-byte sector in
+                        // one 256-bit store (coils past the batch hold the zero
+                        // rows of V)
+                        if (e * 4 < cact)
+                            asm volatile("st.global.cs.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(
+                                             part + pp * sh.ccp + e * 4),
+                                         "f"(v[0].x), "f"(v[0].y), "f"(v[1].x), "f"(v[1].y), "f"(v[2].x), "f"(v[2].y),
+                                         "f"(v[3].x), "f"(v[3].y)
+                                         : "memory");
                     } else {
 #pragma unroll
                         for (int cc = 0; cc < 4; cc++) {
@@ -717,6 +722,36 @@ __device__ __forceinline__ uint4 tm_cover(int pos, int G, int T, int R, int half
     return make_uint4(e[0], e[1], e[2], e[3]);
 }
 
+__device__ __forceinline__ int tm_cover_count(const uint4 &c)
+{
+    const uint32_t w[4] = {c.x, c.y, c.z, c.w};
+    int n = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) n += ((w[q] & 0xffffu) != 0) + ((w[q] >> 16) != 0);
+    return n;
+}
+
+// 8 coils of one region point of a deterministic scratch slot (64 contiguous
+// bytes, two 256-bit loads), and their addition to the accumulators
+__device__ __forceinline__ void tm_ld8(const float2 *src, float (&v)[16])
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(src));
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "l"(src + 4));
+}
+
+__device__ __forceinline__ void tm_add8(float2 (&acc)[8], const float (&v)[16])
+{
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        acc[c].x += v[2 * c];
+        acc[c].y += v[2 * c + 1];
+    }
+}
+
 __device__ __forceinline__ int tm_cover_at(const uint4 &c, int k)
 {
     const int q = k >> 1;  // entries 2q and 2q + 1 share a word
@@ -725,18 +760,19 @@ __device__ __forceinline__ int tm_cover_at(const uint4 &c, int k)
 }
 
 // Deterministic mode: every grid point adds, for kTmGatherCoils coils of one
-// coil chunk (blockIdx.y: chunk, coil group), in a fixed order (covering bins
-// by z, y, x offset, then each bin's items in sample order) the partial sums
-// that the covering items stored in their scratch slots, and writes the grid
-// once (0 where no item covers it). Lanes run along x, so a warp reads groups
-// of neighbouring region points of a few slots and writes 32 neighbouring
-// grid points per coil; the coil groups run one after another over the grid,
-// so the slots that one grid plane reads stay in L2 between its rows. The
-// cover lists of all positions (two entries per 32-bit word, up to 8 per
+// coil chunk, in a fixed order (covering bins by z, y, x offset, then each
+// bin's items in sample order) the partial sums that the covering items
+// stored in their scratch slots ([region point][coil]), and writes the grid
+// once (0 where no item covers it). A thread reads its coils of a region
+// point as 64 contiguous bytes; lanes run along x, so a warp writes 32
+// neighbouring grid points per coil. The coil groups of the same points are
+// neighbouring blocks (blockIdx.x = point block * groups + group, blockIdx.y
+// = chunk), so each point's coils (256 bytes of a slot) come from DRAM once.
+// The cover lists of all positions (two entries per 32-bit word, up to 8 per
 // position) are built per block in shared memory (G[0] + G[1] + G[2] uint4).
 constexpr int kTmGatherCoils = 8;
 
-__global__ void __launch_bounds__(256) grid_tm_gather_kernel(Geom g, TmShape sh, const int32_t *__restrict__ istart,
+__global__ void __launch_bounds__(256, 2) grid_tm_gather_kernel(Geom g, TmShape sh, const int32_t *__restrict__ istart,
                                                             const float2 *__restrict__ scratch,
                                                             float2 *__restrict__ grid, int64_t batch, int nchunks)
 {
@@ -747,43 +783,78 @@ __global__ void __launch_bounds__(256) grid_tm_gather_kernel(Geom g, TmShape sh,
             cov[a][pos] = tm_cover(pos, g.G[a], g.T[a], sh.R[a], g.half[a]);
     __syncthreads();
     const int ngrp = (sh.CC + kTmGatherCoils - 1) / kTmGatherCoils;
-    const int cch = blockIdx.y / ngrp, c0 = (blockIdx.y % ngrp) * kTmGatherCoils;
+    const int cch = blockIdx.y, c0 = (blockIdx.x % ngrp) * kTmGatherCoils;
+    const int pblock = blockIdx.x / ngrp, pblocks = gridDim.x / ngrp;
     const int64_t b0 = (int64_t)cch * sh.CC + c0;
     // coils of this chunk (the last chunk may hold fewer than CC), of this group
     const int ccoils = (int)min((int64_t)sh.CC, batch - (int64_t)cch * sh.CC);
     const int cact = min(kTmGatherCoils, ccoils - c0);
     const int64_t npts = (int64_t)g.nframes * g.gsize;
     const int gxy = g.G[0] * g.G[1];
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = (int64_t)pblock * blockDim.x + threadIdx.x; i < npts; i += (int64_t)pblocks * blockDim.x) {
         const int f = (int)(i / g.gsize), r = (int)(i - (int64_t)f * g.gsize);
         const int z = r / gxy, y = (r - z * gxy) / g.G[0], x = r - z * gxy - y * g.G[0];
         const uint4 cz = cov[2][z], cy = cov[1][y], cx = cov[0][x];
         float2 acc[kTmGatherCoils];
 #pragma unroll
         for (int c = 0; c < kTmGatherCoils; c++) acc[c] = make_float2(0.0f, 0.0f);
-        for (int kz = 0; kz < 8; kz++) {
-            const int vz = tm_cover_at(cz, kz);
-            if (vz < 0) break;
-            for (int ky = 0; ky < 8; ky++) {
-                const int vy = tm_cover_at(cy, ky);
-                if (vy < 0) break;
-                const int kyz = f * g.nbins + ((vz >> 3) * g.nb[1] + (vy >> 3)) * g.nb[0];
-                const int pyz = ((vz & 7) * sh.R[1] + (vy & 7)) * sh.R[0];
-                for (int kx = 0; kx < 8; kx++) {
-                    const int vx = tm_cover_at(cx, kx);
-                    if (vx < 0) break;
-                    const int key = kyz + (vx >> 3);
-                    const int s1 = istart[key + 1];
-                    const int pt = pyz + (vx & 7);
-                    for (int s = istart[key]; s < s1; s++) {
-                        const float2 *src = scratch + (((int64_t)s * nchunks + cch) * sh.CC + c0) * kTmN + pt;
+        const int ncz = tm_cover_count(cz), ncy = tm_cover_count(cy), ncx = tm_cover_count(cx);
+        auto slot = [&](int s, int pt) {
+            return scratch + (((int64_t)s * nchunks + cch) * kTmN + pt) * sh.ccp + c0;
+        };
+        if (ncz <= 2 && ncy <= 2 && ncx <= 2) {
+            // at most two covering bins per axis (every position of the usual
+            // geometries): the item ranges of all 8 candidates first, then the
+            // first items of 4 candidates at a time, so that their loads are
+            // in flight together; the additions keep the general order
+            int beg[8], cnt[8], pts[8];
 #pragma unroll
-                        for (int c = 0; c < kTmGatherCoils; c++)
-                            if (c < cact) {
-                                const float2 v = __ldg(src + c * kTmN);
-                                acc[c].x += v.x;
-                                acc[c].y += v.y;
-                            }
+            for (int q = 0; q < 8; q++) {
+                const int kz = q >> 2, ky = (q >> 1) & 1, kx = q & 1;
+                beg[q] = cnt[q] = pts[q] = 0;
+                if (kz < ncz && ky < ncy && kx < ncx) {
+                    const int vz = tm_cover_at(cz, kz), vy = tm_cover_at(cy, ky), vx = tm_cover_at(cx, kx);
+                    const int key = f * g.nbins + ((vz >> 3) * g.nb[1] + (vy >> 3)) * g.nb[0] + (vx >> 3);
+                    beg[q] = __ldg(istart + key);
+                    cnt[q] = __ldg(istart + key + 1) - beg[q];
+                    pts[q] = ((vz & 7) * sh.R[1] + (vy & 7)) * sh.R[0] + (vx & 7);
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                float v[2][16];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+                    if (cnt[2 * h + j] > 0) tm_ld8(slot(beg[2 * h + j], pts[2 * h + j]), v[j]);
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int q = 2 * h + j;
+                    if (cnt[q] > 0) {
+                        tm_add8(acc, v[j]);
+                        for (int s = beg[q] + 1; s < beg[q] + cnt[q]; s++) {
+                            float w[16];
+                            tm_ld8(slot(s, pts[q]), w);
+                            tm_add8(acc, w);
+                        }
+                    }
+                }
+            }
+        } else {
+            for (int kz = 0; kz < ncz; kz++) {
+                const int vz = tm_cover_at(cz, kz);
+                for (int ky = 0; ky < ncy; ky++) {
+                    const int vy = tm_cover_at(cy, ky);
+                    const int kyz = f * g.nbins + ((vz >> 3) * g.nb[1] + (vy >> 3)) * g.nb[0];
+                    const int pyz = ((vz & 7) * sh.R[1] + (vy & 7)) * sh.R[0];
+                    for (int kx = 0; kx < ncx; kx++) {
+                        const int vx = tm_cover_at(cx, kx);
+                        const int key = kyz + (vx >> 3);
+                        const int s1 = istart[key + 1];
+                        for (int s = istart[key]; s < s1; s++) {
+                            float w[16];
+                            tm_ld8(slot(s, pyz + (vx & 7)), w);
+                            tm_add8(acc, w);
+                        }
                     }
                 }
             }
@@ -805,6 +876,7 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
     s.vrows = s.R[0] + s.R[1] + s.R[2];
     if (s.vrows > kTmMaxRows) return false;
     s.CC = (int)std::min<int64_t>(batch, kTmCC);
+    s.ccp = (s.CC + 7) / 8 * 8;
     s.wp = p->tg_wp;
     int off = kTmSB * 3 * s.wp * 4;  // tap weights of the pass, [sample][axis][wp]
     s.l_off = off;
@@ -844,12 +916,13 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
 // when the plan has none or the geometry does not fit (the caller then uses
 // the other kernels).
 // scratch of deterministic tensor-core gridding: one slot of kTmN region
-// points per (work item, coil)
+// points per (work item, coil chunk), each point the chunk's coils rounded up
+// to 8
 size_t tm_scratch_bytes(const dmr_plan *p, int64_t batch)
 {
     if (p->g.ndim != 3 || p->tg_T[0] == 0 || p->tg_nwork == 0 || batch < 1) return 0;
     const int64_t cc = std::min<int64_t>(batch, kTmCC);
-    return (size_t)p->tg_nwork * ceil_div(batch, cc) * cc * kTmN * sizeof(float2);
+    return (size_t)p->tg_nwork * ceil_div(batch, cc) * kTmN * ((cc + 7) / 8 * 8) * sizeof(float2);
 }
 
 int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
@@ -901,7 +974,7 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     // (no grid writes), then the gather sums them per grid point in a fixed
     // order: every run adds the same values in the same order
     const int ngrp = (sh.CC + kTmGatherCoils - 1) / kTmGatherCoils;
-    DMR_CHECK(nchunks * ngrp <= 65535, DMR_ERR_UNSUPPORTED, "batch too large");
+    DMR_CHECK(nchunks <= 65535, DMR_ERR_UNSUPPORTED, "batch too large");
     // the gather's cover lists: one uint4 per grid position of each axis
     const size_t gsmem = (size_t)(p->g.G[0] + p->g.G[1] + p->g.G[2]) * sizeof(uint4);
     if (gsmem > 48 * 1024) {
@@ -927,7 +1000,7 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     if (rc == DMR_OK) {
         const int64_t npts = (int64_t)g.nframes * g.gsize;
         const int gblocks = (int)std::min<int64_t>(ceil_div(npts, 256), (int64_t)sms * 16);
-        grid_tm_gather_kernel<<<dim3(gblocks, (unsigned)(nchunks * ngrp)), 256, gsmem, st>>>(
+        grid_tm_gather_kernel<<<dim3(gblocks * ngrp, (unsigned)nchunks), 256, gsmem, st>>>(
             g, sh, p->tg_item_start, (const float2 *)scratch, grid, batch, (int)nchunks);
         g_launches.fetch_add(1, std::memory_order_relaxed);
         e = cudaGetLastError();
