@@ -36,6 +36,7 @@ SYMBOLS = (
     "dmr_tc_test_stall",
     "dmr_fft3_fused",
     "dmr_tc_min_coils",
+    "dmr_scratch_release",
     "dmr_detect_cartesian",
     "dmr_plan_create",
     "dmr_plan_destroy",
@@ -90,6 +91,7 @@ _SIGS = {
     "dmr_tc_test_stall": (ctypes.c_int, [ctypes.c_int]),
     "dmr_fft3_fused": (ctypes.c_int, [vp]),
     "dmr_tc_min_coils": (ctypes.c_int, [ctypes.c_int]),
+    "dmr_scratch_release": (ctypes.c_int, [ctypes.c_int]),
     "dmr_detect_cartesian": (ctypes.c_int, [vp, i64, ctypes.c_int, i32p, i32p, vp]),
     "dmr_plan_create": (
         ctypes.c_int,

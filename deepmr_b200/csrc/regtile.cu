@@ -597,14 +597,17 @@ size_t rt_scratch_bytes(const dmr_plan *p, int64_t batch)
     return (size_t)p->rt_slots * ncc * kRtPts * kRtCoils * sizeof(float2);
 }
 
-// Library-owned stream-ordered pool for the scratch of calls without a workspace.
-cudaMemPool_t scratch_pool(int dev)
+// Library-owned stream-ordered pool for the scratch of calls without a
+// workspace (created on first use unless `create` is false; nullptr then).
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static cudaMemPool_t find_pool(int dev, bool create)
 {
-    static std::mutex mu;
-    static std::map<int, cudaMemPool_t> pools;
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = pools.find(dev);
-    if (it != pools.end()) return it->second;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) return it->second;
+    if (!create) return nullptr;
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -616,9 +619,11 @@ cudaMemPool_t scratch_pool(int dev)
     }
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    pools[dev] = pool;
+    g_pools[dev] = pool;
     return pool;
 }
+
+cudaMemPool_t scratch_pool(int dev) { return find_pool(dev, true); }
 
 template <int W>
 static int rt_launch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
@@ -678,3 +683,18 @@ int grid_rt_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
 }
 
 }  // namespace dmr
+
+// Return the scratch pool's free memory on `device` to the device.
+extern "C" int dmr_scratch_release(int device)
+{
+    cudaMemPool_t pool = dmr::find_pool(device, false);
+    if (!pool) return DMR_OK;
+    int old = 0;
+    DMR_CUDA(cudaGetDevice(&old));
+    DMR_CUDA(cudaSetDevice(device));
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+    cudaSetDevice(old);
+    if (e != cudaSuccess) return dmr::cuda_fail(e, "dmr_scratch_release", __FILE__, __LINE__);
+    return DMR_OK;
+}

@@ -45,6 +45,7 @@ __all__ = [
     "GramMatrix",
     "set_deterministic_gridding",
     "deterministic_gridding",
+    "release_scratch",
     "set_status_check",
     "traj_grad",
     "CapturedNUFFT",
@@ -64,10 +65,12 @@ __all__ = [
 def set_deterministic_gridding(flag=True):
     """Select the gridding kernel used by the adjoint NUFFT.
 
-    True: bitwise reproducible — 3D plans grid on the tensor cores in colour
-    launches (no two bins of a launch share a grid point; bins of more than
-    2048 samples are split into segments whose partial sums are added in a
-    fixed order), other plans with one owner per grid point or per tile.
+    True: bitwise reproducible — 3D plans grid on the tensor cores with
+    every work item (a bin, or 2048 samples of a heavier one) storing its
+    region's partial sums, which a gather then adds per grid point in a fixed
+    order (the partial sums take 2 KB per work item and coil in the library's
+    scratch pool: see release_scratch); other plans with one owner per grid
+    point or per tile.
     False (default): grid-point additions with atomics (summation order may
     vary between runs, results agree to float32 rounding).
     Returns the previous setting.
@@ -75,6 +78,22 @@ def set_deterministic_gridding(flag=True):
     old = _nufft.DETERMINISTIC_GRIDDING
     _nufft.DETERMINISTIC_GRIDDING = bool(flag)
     return old
+
+
+def release_scratch(device=None):
+    """Give the memory that the library's scratch pool holds beyond what is in
+    use back to the device (default: the current CUDA device). Synchronises
+    the device."""
+    import torch
+
+    from .. import _lib
+
+    if isinstance(device, int):
+        dev = device
+    else:
+        idx = None if device is None else torch.device(device).index
+        dev = torch.cuda.current_device() if idx is None else idx
+    _lib.check(_lib.lib().dmr_scratch_release(int(dev)))
 
 
 def deterministic_gridding():

@@ -106,6 +106,17 @@ int dmr_fft3_fused(dmr_plan *plan);
 int dmr_tc_min_coils(int coils);
 
 /*
+ * Housekeeping, no reference counterpart: gives back to `device` the memory
+ * that the library's scratch pool holds beyond what is in use. Calls without
+ * a large enough workspace take their gridding scratch from this pool, which
+ * keeps it for the next call; deterministic 3D gridding keeps every work
+ * item's partial sums there (2 KB per gridding work item and coil: 13.6 GB
+ * for 32 coils of the 192^3, 19.2 M-sample kooshball). Synchronises the
+ * device first. Returns 0 or a DMR_ERR_* code.
+ */
+int dmr_scratch_release(int device);
+
+/*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
  * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
  * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the

@@ -7,9 +7,9 @@ oversampling 1.25, 32 coils on the GPU. Coils are independent, so coils 0 and
 coils alone (the oracle restates the reference's CPU loops,
 src/deepmr/fft/_interp/interp.py:124-227 and grid.py:181-284). Checked: the
 forward (interpolation), the atomic adjoint (tensor-core gridding) and the
-deterministic adjoint (tensor-core gridding in colour launches over rows of
-bins, one block adding a row's bins in x order and the kooshball centre's bins
-as consecutive segments; two calls bitwise equal), plus independence of the
+deterministic adjoint (tensor-core gridding into per-item partial sums, the
+kooshball centre's bins as several 2048-sample items, gathered per grid point
+in a fixed order; two calls bitwise equal), plus independence of the
 result from the coil count (the tensor-core kernel's block shape depends on
 it). This covers the kooshball centre's bins split into several work items,
 the work-item order in 4x4x4-bin tiles and sample indices near 2^24.

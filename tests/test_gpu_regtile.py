@@ -1,6 +1,7 @@
 """GPU parity of deterministic 3D gridding against the oracle: the tensor-core
-kernel in colour launches for widths 2..5 (heavy bins split into segments
-whose partial sums a reduction adds in order), the register-tile kernel for
+kernel for widths 2..5 (every work item, a bin or a 2048-sample segment of a
+heavier one, stores its region's partial sums; a gather adds them per grid
+point in a fixed order), the register-tile kernel for
 wider kernels and when the tensor-core path is switched off (DMR_NO_TC=1, in
 a child process): regular and anisotropic grids (partial block regions at
 the grid edge), several widths, coil counts that leave part of a 32-coil
