@@ -21,6 +21,9 @@ def golden_cases(prefix=None, kind="nufft"):
     sparse = [n for n in names if n.startswith("sparse")]
     cgsense = [n for n in names if n.startswith("cgsense")]
     calib = [n for n in names if n.startswith("calib")]
+    dcf = [n for n in names if n.startswith("dcf")]
+    if kind == "dcf":
+        return dcf
     if kind == "cgsense":
         return cgsense
     if kind == "calib":
@@ -31,7 +34,7 @@ def golden_cases(prefix=None, kind="nufft"):
         return lowrank
     if kind == "sparse":
         return sparse
-    other = set(toep) | set(lowrank) | set(sparse) | set(cgsense) | set(calib)
+    other = set(toep) | set(lowrank) | set(sparse) | set(cgsense) | set(calib) | set(dcf)
     return [n for n in names if n not in other]
 
 

@@ -9,6 +9,7 @@ the ``DEEPMR_REFERENCE`` environment variable (the project root, containing
     python tests/golden/make_golden.py sparse     # only the sparse FFT cases
     python tests/golden/make_golden.py cgsense    # only the CG-SENSE case
     python tests/golden/make_golden.py calib      # only the calibration cases
+    python tests/golden/make_golden.py dcf        # only the Voronoi density cases
 
 The reference's top-level package import needs optional I/O dependencies that
 are absent, so the script registers stub parent packages whose ``__path__``
@@ -144,6 +145,49 @@ def import_reference_calib():
     import deepmr.recon.calib.espirit as espirit  # noqa: E402
 
     return acs, espirit
+
+
+def import_reference_dcf():
+    """The reference's density compensation module
+    (src/deepmr/_design/grad/utils/dcf.py) through stub parents (its package
+    __init__ files import the whole design toolbox)."""
+    import_reference()
+    for name, sub in [("deepmr._design", "/_design"), ("deepmr._design.grad", "/_design/grad"),
+                      ("deepmr._design.grad.utils", "/_design/grad/utils")]:
+        mod = types.ModuleType(name)
+        mod.__path__ = [REF_SRC + sub]
+        sys.modules[name] = mod
+    import deepmr._design.grad.utils.dcf as dcf  # noqa: E402
+
+    return dcf
+
+
+def dcf_cases():
+    """Voronoi density compensation (src/deepmr/_design/grad/utils/dcf.py:75-160)
+    on float32 trajectories:
+    dcf_radial2d: 2D radial, 24 spokes x 33 samples through k = 0 (the centre
+    repeated 24 times), ratio 0.1;
+    dcf_spiral_shots: one 400-sample spiral interleaf as 6 uniformly rotated
+    shots (nshots = 6; the shots share k = 0);
+    dcf_spiral_edge: 4 rotated 300-sample interleaves, fix_edge, ratio 0.2;
+    dcf_koosh3d: 3D golden-means kooshball, 60 spokes x 12 samples."""
+    dcf = import_reference_dcf()
+    cases = {}
+    ang = np.pi * np.arange(24) / 24
+    r = np.linspace(-16, 16, 33)
+    c = np.stack([np.outer(np.cos(ang), r), np.outer(np.sin(ang), r)], axis=-1).astype(np.float32)
+    cases["dcf_radial2d"] = (c, dict(nshots=1, fix_edge=False, ratio=0.1))
+    c = synth.spiral_2d(400, 48, nturns=6)[0]
+    cases["dcf_spiral_shots"] = (c, dict(nshots=6, fix_edge=False, ratio=0.1))
+    c = np.concatenate([synth.spiral_2d(300, 40, rotation=0.5 * np.pi * s, nturns=5) for s in range(4)])
+    cases["dcf_spiral_edge"] = (c, dict(nshots=1, fix_edge=True, ratio=0.2))
+    c = synth.kooshball_3d(60, 12, 16)
+    cases["dcf_koosh3d"] = (c, dict(nshots=1, fix_edge=False, ratio=0.1))
+    for name, (c, kw) in cases.items():
+        w = dcf.voronoi(np.array(c, copy=True), **kw)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), coord=c, dcf=np.asarray(w),
+                            nshots=kw["nshots"], fix_edge=kw["fix_edge"], ratio=kw["ratio"])
+        print("wrote", name, np.asarray(w).shape)
 
 
 def calib_cases(seed=0):
@@ -367,6 +411,9 @@ def main():
     if sys.argv[1:] == ["sparse"]:
         sparse_cases()
         return
+    if sys.argv[1:] == ["dcf"]:
+        dcf_cases()
+        return
     if sys.argv[1:] == ["calib"]:
         calib_cases()
         return
@@ -434,6 +481,7 @@ def main():
     sparse_cases()
     cgsense_case()
     calib_cases()
+    dcf_cases()
 
 
 if __name__ == "__main__":
