@@ -40,8 +40,17 @@ namespace {
 #ifndef DMR_FFT_LINES
 #define DMR_FFT_LINES 16
 #endif
+// resident blocks per SM the compiler plans registers for: the row and column
+// passes of blocks of at most 256 threads at 3 (about 80 registers; 39.5 vs
+// 39.9 ms per 240^3 x 32 forward + adjoint pair at 2), larger blocks (a factor
+// above 16: 320 or 384 threads) at 2, where 3 would cap them at 56-64
+// registers and spill; the fused Toeplitz z pass at 2 (its forward transform,
+// kernel multiply and inverse transform need the registers)
 #ifndef DMR_FFT_MINB
-#define DMR_FFT_MINB 2
+#define DMR_FFT_MINB 3
+#endif
+#ifndef DMR_FFT_TOEP_MINB
+#define DMR_FFT_TOEP_MINB 2
 #endif
 constexpr int kFftLines = DMR_FFT_LINES;  // lines per block (16 or 32)
 constexpr int kFftLP = kFftLines + 2;     // shared-memory pitch of a position (16-byte rows)
@@ -202,6 +211,7 @@ struct Len {
     static constexpr int L = L_, L1 = L1_, L2 = L2_;
     // one thread per (line, column) of step A and per (line, row) of step B
     static constexpr int T = kFftLines * (L1 > L2 ? L1 : L2);
+    static constexpr int MINB = T <= 256 ? DMR_FFT_MINB : 2;
     static_assert(L1 * L2 == L, "factors");
 };
 
@@ -359,7 +369,7 @@ __device__ __forceinline__ void row_lines(const FftGeom &g, int64_t row0, int64_
 //   adjoint (CROP true): grid rows are inverse-transformed and the kept x,
 //   scaled and apodised, written to the image.
 template <class F, bool CROP>
-__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_rows_kernel(FftGeom g, const float2 *__restrict__ tw,
+__global__ void __launch_bounds__(F::T, F::MINB) fft_rows_kernel(FftGeom g, const float2 *__restrict__ tw,
                                                         const void *__restrict__ src, int src_real,
                                                         float2 *__restrict__ dst)
 {
@@ -482,7 +492,7 @@ struct ColArgs {
 };
 
 template <class F, bool IN_ALL, bool OUT_ALL>
-__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_cols_kernel(FftGeom g, ColArgs a, const float2 *__restrict__ tw,
+__global__ void __launch_bounds__(F::T, F::MINB) fft_cols_kernel(FftGeom g, ColArgs a, const float2 *__restrict__ tw,
                                                         float2 *grid)
 {
     constexpr int L = F::L, L1 = F::L1, L2 = F::L2, T = F::T;
@@ -557,7 +567,7 @@ __global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_cols_kernel(FftGeom g,
 // memory between the two transforms. Tiles run batch-fastest, so the blocks
 // that read one kernel tile run together and share it in L2.
 template <class F>
-__global__ void __launch_bounds__(F::T, DMR_FFT_MINB) fft_toep_z_kernel(FftGeom g, ColArgs a, int64_t nk,
+__global__ void __launch_bounds__(F::T, DMR_FFT_TOEP_MINB) fft_toep_z_kernel(FftGeom g, ColArgs a, int64_t nk,
                                                           const float2 *__restrict__ kern, float kscale,
                                                           const float2 *__restrict__ tw, float2 *grid)
 {
