@@ -37,6 +37,7 @@ SYMBOLS = (
     "dmr_fft3_fused",
     "dmr_tc_min_coils",
     "dmr_scratch_release",
+    "dmr_det_scratch_limit",
     "dmr_detect_cartesian",
     "dmr_plan_create",
     "dmr_plan_destroy",
@@ -92,6 +93,7 @@ _SIGS = {
     "dmr_fft3_fused": (ctypes.c_int, [vp]),
     "dmr_tc_min_coils": (ctypes.c_int, [ctypes.c_int]),
     "dmr_scratch_release": (ctypes.c_int, [ctypes.c_int]),
+    "dmr_det_scratch_limit": (ctypes.c_int64, [ctypes.c_int64]),
     "dmr_detect_cartesian": (ctypes.c_int, [vp, i64, ctypes.c_int, i32p, i32p, vp]),
     "dmr_plan_create": (
         ctypes.c_int,

@@ -104,11 +104,13 @@ int grid_tc_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *gr
 // tensor-core gridding with the plan's gridding bins (tmgrid.cu), atomic or
 // deterministic (partial sums per work item, then a gather per grid point;
 // scratch from the caller when it holds tm_scratch_bytes, else from the
-// library pool); `timeouts` is the device
+// library pool; DMR_ERR_UNSUPPORTED, before any launch, when it needs more
+// than `det_limit` bytes (> 0) or the pool has no memory for it, so that the
+// caller takes another deterministic kernel); `timeouts` is the device
 // address of the process-wide counter of blocks that stopped on a bounded wait
 int grid_tm_dispatch(const ::dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes, int *timeouts,
-                     int stall, cudaStream_t st);
+                     int stall, int64_t det_limit, cudaStream_t st);
 
 }  // namespace dmr
 

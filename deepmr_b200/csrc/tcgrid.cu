@@ -33,6 +33,9 @@ static int tc_disabled()
 }
 
 static std::atomic<int> g_tc_stall{0};  // test hook (dmr_tc_test_stall)
+// largest scratch (bytes) deterministic tensor-core gridding may take, 0: no
+// limit (dmr_det_scratch_limit)
+static std::atomic<int64_t> g_det_scratch_max{0};
 
 // device address of g_tc_timeouts, looked up once per device (that device current)
 static int timeouts_ptr(int dev, int **out)
@@ -59,7 +62,7 @@ int grid_tc_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
     int *timeouts = nullptr;
     DMR_TRY(timeouts_ptr(dev, &timeouts));
     return grid_tm_dispatch(p, ksp, kreal, grid, batch, weight, wpb, det, scratch, scratch_bytes, timeouts,
-                            g_tc_stall.load(), st);
+                            g_tc_stall.load(), g_det_scratch_max.load(), st);
 }
 
 }  // namespace dmr
@@ -78,6 +81,11 @@ extern "C" int dmr_tc_timeouts(int64_t *count, int reset)
         DMR_CUDA(cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)));
     }
     return DMR_OK;
+}
+
+extern "C" int64_t dmr_det_scratch_limit(int64_t bytes)
+{
+    return bytes >= 0 ? g_det_scratch_max.exchange(bytes) : g_det_scratch_max.load();
 }
 
 extern "C" int dmr_tc_test_stall(int enable)

@@ -927,7 +927,7 @@ size_t tm_scratch_bytes(const dmr_plan *p, int64_t batch)
 
 int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
                      const float *weight, int wpb, int det, void *scratch, size_t scratch_bytes, int *timeouts,
-                     int stall, cudaStream_t st)
+                     int stall, int64_t det_limit, cudaStream_t st)
 {
     int dev = 0, sms = 0, smem_blk = 0;
     DMR_CUDA(cudaGetDevice(&dev));
@@ -982,11 +982,19 @@ int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid
         DMR_CUDA(cudaFuncSetAttribute(grid_tm_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem));
     }
     const size_t need = tm_scratch_bytes(p, batch);
+    // over the caller's limit, or no memory for it: another deterministic
+    // kernel takes the call (nothing has been launched yet)
+    if (det_limit > 0 && need > (size_t)det_limit) return DMR_ERR_UNSUPPORTED;
     void *owned = nullptr;
     if (scratch == nullptr || scratch_bytes < need) {
         cudaMemPool_t pool = scratch_pool(p->device);
-        DMR_CHECK(pool != nullptr, DMR_ERR_CUDA, "no memory pool for the gridding scratch");
-        DMR_CUDA(cudaMallocFromPoolAsync(&owned, need, pool, st));
+        if (pool == nullptr) return DMR_ERR_UNSUPPORTED;
+        const cudaError_t e = cudaMallocFromPoolAsync(&owned, need, pool, st);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return DMR_ERR_UNSUPPORTED;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
         scratch = owned;
     }
     int rc = DMR_OK;

@@ -46,6 +46,7 @@ __all__ = [
     "set_deterministic_gridding",
     "deterministic_gridding",
     "release_scratch",
+    "set_deterministic_scratch_limit",
     "set_status_check",
     "traj_grad",
     "CapturedNUFFT",
@@ -94,6 +95,19 @@ def release_scratch(device=None):
         idx = None if device is None else torch.device(device).index
         dev = torch.cuda.current_device() if idx is None else idx
     _lib.check(_lib.lib().dmr_scratch_release(int(dev)))
+
+
+def set_deterministic_scratch_limit(nbytes):
+    """Largest scratch (bytes) that deterministic 3D tensor-core gridding may
+    take (2 KB per gridding work item and coil); a call that would need more,
+    or for which the device has no memory left, runs on the register-tile
+    kernel instead (deterministic, slower, small scratch). 0 removes the
+    limit (the default). Process-wide; returns the previous limit."""
+    from .. import _lib
+
+    if nbytes < 0:
+        raise ValueError("nbytes must be >= 0")
+    return int(_lib.lib().dmr_det_scratch_limit(int(nbytes)))
 
 
 def deterministic_gridding():

@@ -117,6 +117,17 @@ int dmr_tc_min_coils(int coils);
 int dmr_scratch_release(int device);
 
 /*
+ * Memory control, no reference counterpart: the largest scratch, in bytes,
+ * that deterministic 3D tensor-core gridding may take (its per-item partial
+ * sums, 2 KB per gridding work item and coil). A call that would need more,
+ * or for which the pool has no memory, runs on the register-tile kernel (or
+ * the colour passes) instead: deterministic as well, slower, with a small
+ * scratch. bytes > 0 sets the limit, 0 removes it (the default), < 0 only
+ * queries. Returns the previous limit. Process-wide.
+ */
+int64_t dmr_det_scratch_limit(int64_t bytes);
+
+/*
  * Cartesian-axis test of plan_nufft (src/deepmr/fft/nufft.py:104-109):
  * for coordinate axis a (x, y, z order), all(|s - round(s)| <= 1e-8 + 1e-5|round(s)|)
  * in float32 with s = shape_zyx[a] * coord[..., a] (the reference pairs the

@@ -119,6 +119,33 @@ def test_tc_grid_deterministic_vs_oracle_and_release(F, ncoils):
     assert torch.equal(x, _grid(F, plan, ksp.cuda(), dcf.cuda(), det=True))
 
 
+def test_tc_grid_deterministic_scratch_limit_falls_back(F):
+    """A scratch limit below what deterministic tensor-core gridding needs
+    sends the call to the register-tile kernel: within 1e-5 of the oracle,
+    bitwise reproducible, and not bitwise equal to the tensor-core result
+    (another summation order), which shows that the other kernel ran."""
+    from oracle import nufft_ref as R
+    from deepmr_b200 import synth
+
+    n = 20
+    coord = synth.kooshball_3d(300, 2 * n, n).astype(np.float32)
+    c = torch.as_tensor(coord)
+    plan = F.plan_nufft(c, n, 4, 1.25, device="cuda")
+    ksp = synth.complex_gaussian((12,) + coord.shape[:-1], seed=31)
+    ref = R.apply_nufft_adj(ksp, R.plan_nufft(c, n, 4, 1.25))
+    old = F.set_deterministic_scratch_limit(1)
+    try:
+        assert F.set_deterministic_scratch_limit(1) == 1
+        x = _grid(F, plan, ksp.cuda(), det=True)
+        x2 = _grid(F, plan, ksp.cuda(), det=True)
+    finally:
+        F.set_deterministic_scratch_limit(old)
+    xt = _grid(F, plan, ksp.cuda(), det=True)
+    assert rel(x, ref) < TOL and rel(xt, ref) < TOL
+    assert torch.equal(x, x2)
+    assert not torch.equal(x, xt)
+
+
 def test_tc_grid_adjoint_identity(F):
     """<A x, y> = G <x, A^H y> with the tensor-core adjoint."""
     from deepmr_b200 import synth
