@@ -70,7 +70,10 @@ constexpr int kTmValueWarp = kTmMmaWarp + 1;
 constexpr int kTmThreads = (kTmValueWarp + 1) * 32;
 constexpr int kTmEpi = 256;
 constexpr int kTmMaxRows = 24;             // region rows over the three axes (7 + 6 + 6 = 19 used)
-constexpr int kTmTable = kTmMaxRows * 8;   // a chunk's weight table: rows x 8 samples
+// a chunk's weight table: rows of 8 samples, 12 floats apart (48 bytes: the
+// 16-byte reads of up to 8 consecutive rows fall on disjoint banks)
+constexpr int kTmTableRow = 12;
+constexpr int kTmTable = kTmMaxRows * kTmTableRow;
 constexpr int kTmSC = 8;                   // samples per chunk (K of one tf32 MMA)
 constexpr int kTmSB = 128;                 // samples per pass
 // samples accumulated in tensor memory before a read-back: the fp32 sums of
@@ -316,9 +319,9 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
             const int pc = min(p, sh.P - 1);
             const int rz = pc / RXY, rem = pc - rz * RXY;
             const int ry = rem / sh.R[0], rx = rem - ry * sh.R[0];
-            vxyz[h][0] = (uint32_t)rx * 32;  // table rows of 8 floats
-            vxyz[h][1] = (uint32_t)(sh.R[0] + ry) * 32;
-            vxyz[h][2] = (uint32_t)(sh.R[0] + sh.R[1] + rz) * 32;
+            vxyz[h][0] = (uint32_t)rx * (4 * kTmTableRow);  // table rows
+            vxyz[h][1] = (uint32_t)(sh.R[0] + ry) * (4 * kTmTableRow);
+            vxyz[h][2] = (uint32_t)(sh.R[0] + sh.R[1] + rz) * (4 * kTmTableRow);
             woff[h] = tm_off(p, 0);  // and + 128 for samples 4..7
         }
         const int bs = btid & 7;
@@ -386,7 +389,7 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                         const int i = trow_r[h] - ((pl[si] >> (8 * a)) & 255);
                         if (i >= 0 && i < W) v = pw[(si * 3 + a) * sh.wp + i];
                     }
-                    table[e] = v;
+                    table[(e >> 3) * kTmTableRow + (e & 7)] = v;
                 }
                 // the group's barrier: the table is complete, and the group leaves
                 // together if a wait ran out (nothing asynchronous was written yet)
@@ -431,10 +434,14 @@ __global__ void __launch_bounds__(kTmThreads, 1) grid_tmem_kernel(
                         }
                     }
                     const float hx = tc_hi(v.x), hy = tc_hi(v.y);
-                    tc_sts(sbase + tm_off(2 * bc, bs), hx);
-                    tc_sts(sbase + tm_off(2 * bc + 1, bs), hy);
-                    tc_sts(sbase + tm_off(64 + 2 * bc, bs), v.x - hx);
-                    tc_sts(sbase + tm_off(65 + 2 * bc, bs), v.y - hy);
+                    // samples 4..7 (128 bytes further, the same banks) store the
+                    // imaginary row first, so that each store of the warp
+                    // covers all 32 banks once
+                    const int sw = bs >> 2;
+                    tc_sts(sbase + tm_off(2 * bc + sw, bs), sw ? hy : hx);
+                    tc_sts(sbase + tm_off(2 * bc + 1 - sw, bs), sw ? hx : hy);
+                    tc_sts(sbase + tm_off(64 + 2 * bc + sw, bs), sw ? v.y - hy : v.x - hx);
+                    tc_sts(sbase + tm_off(65 + 2 * bc - sw, bs), sw ? v.x - hx : v.y - hy);
                 }
                 if (btid == 0)
                     stage_meta[stage] = (first ? kChunkFirst : 0u) | (last ? kChunkLast : 0u) |
