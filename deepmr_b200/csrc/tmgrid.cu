@@ -110,7 +110,7 @@ struct TmShape {
     int R[3];        // region extents (tile + W - 1)
     int P;           // region points (<= 256)
     int CC;          // coils per block (<= 32)
-    int ccp;         // deterministic scratch: coil stride of a region point (CC rounded up to 8)
+    int ccp;         // deterministic scratch: coil stride of a region point (CC rounded up to the gather's group)
     int vrows;       // R[0] + R[1] + R[2]
     int table_off;   // per builder group two chunk weight tables (offset in dynamic shared memory)
     int goff_off;    // read-back: grid offsets of the current item's region points
@@ -738,22 +738,24 @@ __device__ __forceinline__ int tm_cover_count(const uint4 &c)
     return n;
 }
 
-// 8 coils of one region point of a deterministic scratch slot (64 contiguous
-// bytes, two 256-bit loads), and their addition to the accumulators
-__device__ __forceinline__ void tm_ld8(const float2 *src, float (&v)[16])
-{
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
-        : "l"(src));
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
-        : "l"(src + 4));
-}
-
-__device__ __forceinline__ void tm_add8(float2 (&acc)[8], const float (&v)[16])
+// G coils of one region point of a deterministic scratch slot (8 G
+// contiguous bytes, 256-bit loads), and their addition to the accumulators
+template <int G>
+__device__ __forceinline__ void tm_ldg(const float2 *src, float (&v)[2 * G])
 {
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
+    for (int j = 0; j < G / 4; j++)
+        asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=f"(v[8 * j]), "=f"(v[8 * j + 1]), "=f"(v[8 * j + 2]), "=f"(v[8 * j + 3]), "=f"(v[8 * j + 4]),
+              "=f"(v[8 * j + 5]), "=f"(v[8 * j + 6]), "=f"(v[8 * j + 7])
+            : "l"(src + 4 * j));
+}
+
+template <int G>
+__device__ __forceinline__ void tm_addg(float2 (&acc)[G], const float (&v)[2 * G])
+{
+#pragma unroll
+    for (int c = 0; c < G; c++) {
         acc[c].x += v[2 * c];
         acc[c].y += v[2 * c + 1];
     }
@@ -771,7 +773,7 @@ __device__ __forceinline__ int tm_cover_at(const uint4 &c, int k)
 // bin's items in sample order) the partial sums that the covering items
 // stored in their scratch slots ([region point][coil]), and writes the grid
 // once (0 where no item covers it). A thread reads its coils of a region
-// point as 64 contiguous bytes; lanes run along x, so a warp writes 32
+// point as 8 kTmGatherCoils contiguous bytes; lanes run along x, so a warp writes 32
 // neighbouring grid points per coil. The coil groups of the same points are
 // neighbouring blocks (blockIdx.x = point block * groups + group, blockIdx.y
 // = chunk), so each point's coils (256 bytes of a slot) come from DRAM once.
@@ -829,19 +831,19 @@ __global__ void __launch_bounds__(256, 2) grid_tm_gather_kernel(Geom g, TmShape 
             }
 #pragma unroll
             for (int h = 0; h < 4; h++) {
-                float v[2][16];
+                float v[2][2 * kTmGatherCoils];
 #pragma unroll
                 for (int j = 0; j < 2; j++)
-                    if (cnt[2 * h + j] > 0) tm_ld8(slot(beg[2 * h + j], pts[2 * h + j]), v[j]);
+                    if (cnt[2 * h + j] > 0) tm_ldg<kTmGatherCoils>(slot(beg[2 * h + j], pts[2 * h + j]), v[j]);
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int q = 2 * h + j;
                     if (cnt[q] > 0) {
-                        tm_add8(acc, v[j]);
+                        tm_addg<kTmGatherCoils>(acc, v[j]);
                         for (int s = beg[q] + 1; s < beg[q] + cnt[q]; s++) {
-                            float w[16];
-                            tm_ld8(slot(s, pts[q]), w);
-                            tm_add8(acc, w);
+                            float w[2 * kTmGatherCoils];
+                            tm_ldg<kTmGatherCoils>(slot(s, pts[q]), w);
+                            tm_addg<kTmGatherCoils>(acc, w);
                         }
                     }
                 }
@@ -858,9 +860,9 @@ __global__ void __launch_bounds__(256, 2) grid_tm_gather_kernel(Geom g, TmShape 
                         const int key = kyz + (vx >> 3);
                         const int s1 = istart[key + 1];
                         for (int s = istart[key]; s < s1; s++) {
-                            float w[16];
-                            tm_ld8(slot(s, pyz + (vx & 7)), w);
-                            tm_add8(acc, w);
+                            float w[2 * kTmGatherCoils];
+                            tm_ldg<kTmGatherCoils>(slot(s, pyz + (vx & 7)), w);
+                            tm_addg<kTmGatherCoils>(acc, w);
                         }
                     }
                 }
@@ -883,7 +885,7 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
     s.vrows = s.R[0] + s.R[1] + s.R[2];
     if (s.vrows > kTmMaxRows) return false;
     s.CC = (int)std::min<int64_t>(batch, kTmCC);
-    s.ccp = (s.CC + 7) / 8 * 8;
+    s.ccp = (s.CC + kTmGatherCoils - 1) / kTmGatherCoils * kTmGatherCoils;
     s.wp = p->tg_wp;
     int off = kTmSB * 3 * s.wp * 4;  // tap weights of the pass, [sample][axis][wp]
     s.l_off = off;
@@ -924,12 +926,13 @@ bool tm_shape(const dmr_plan *p, int64_t batch, int wpb, int smem_limit, TmShape
 // the other kernels).
 // scratch of deterministic tensor-core gridding: one slot of kTmN region
 // points per (work item, coil chunk), each point the chunk's coils rounded up
-// to 8
+// to the gather's coil group
 size_t tm_scratch_bytes(const dmr_plan *p, int64_t batch)
 {
     if (p->g.ndim != 3 || p->tg_T[0] == 0 || p->tg_nwork == 0 || batch < 1) return 0;
     const int64_t cc = std::min<int64_t>(batch, kTmCC);
-    return (size_t)p->tg_nwork * ceil_div(batch, cc) * kTmN * ((cc + 7) / 8 * 8) * sizeof(float2);
+    return (size_t)p->tg_nwork * ceil_div(batch, cc) * kTmN * ((cc + kTmGatherCoils - 1) / kTmGatherCoils * kTmGatherCoils) *
+           sizeof(float2);
 }
 
 int grid_tm_dispatch(const dmr_plan *p, const void *ksp, int kreal, float2 *grid, int64_t batch,
