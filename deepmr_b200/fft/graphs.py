@@ -2,9 +2,10 @@
 
 A captured operator owns static device buffers (input, output, workspace) for
 one plan and batch size; `forward` / `adjoint` copy the caller's data into
-the static input and replay the graph, so a steady-state call is one graph
-launch (the apodise/pad kernel, the cuFFT kernels and the spreading kernel)
-with no host-side argument processing. This replaces the reference's
+the static input (or take what the caller wrote there: `x_in`, `y_in`) and
+replay the graph, so a steady-state call is one graph launch (the FFT passes
+and the interpolation or gridding kernel) with no host-side argument
+processing. This replaces the reference's
 per-call Python dispatch (src/deepmr/fft/nufft.py:450-606) for serving and
 iterative reconstructions that apply the same operator many times.
 """
@@ -83,15 +84,21 @@ class CapturedNUFFT:
                 fn()
         return graph
 
-    def forward(self, image):
-        """image -> kspace (a view of the static output: copy it to keep it)."""
-        self.x_in.copy_(torch.as_tensor(image).reshape(self.image_shape))
+    def forward(self, image=None):
+        """image -> kspace (a view of the static output: copy it to keep it).
+        Without ``image`` (or given ``x_in`` itself) the operator reads what
+        the caller wrote into ``x_in``, and no copy runs."""
+        if image is not None and image is not self.x_in:
+            self.x_in.copy_(torch.as_tensor(image).reshape(self.image_shape))
         self.g_fwd.replay()
         return self.y_out
 
-    def adjoint(self, kspace):
-        """kspace -> image (a view of the static output: copy it to keep it)."""
-        self.y_in.copy_(torch.as_tensor(kspace).reshape(self.kspace_shape))
+    def adjoint(self, kspace=None):
+        """kspace -> image (a view of the static output: copy it to keep it).
+        Without ``kspace`` (or given ``y_in`` itself) the operator reads what
+        the caller wrote into ``y_in``, and no copy runs."""
+        if kspace is not None and kspace is not self.y_in:
+            self.y_in.copy_(torch.as_tensor(kspace).reshape(self.kspace_shape))
         self.g_adj.replay()
         return self.x_out
 

@@ -74,5 +74,10 @@ def test_captured_graph_matches_eager():
             x = op.adjoint(ksp).clone()
             assert torch.equal(y, F.apply_nufft(img, plan, weight=dcf.reshape(c.shape[:-1])))
             assert torch.equal(x, F.apply_nufft_adj(ksp, plan, weight=dcf.reshape(c.shape[:-1])))
+        # inputs written into the static buffers by the caller: no copy, same results
+        op.x_in.copy_(img)
+        op.y_in.copy_(ksp)
+        assert torch.equal(op.forward().clone(), y)
+        assert torch.equal(op.adjoint(op.y_in).clone(), x)
     finally:
         F.set_deterministic_gridding(old)
