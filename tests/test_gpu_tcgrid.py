@@ -60,8 +60,13 @@ def test_tc_grid_vs_oracle(F, ncoils):
     assert rel(x, ref) < TOL
 
 
-@pytest.mark.parametrize("width,os", [(3, 1.25), (4, 1.25), (5, 1.25), (6, 2.0)])
-def test_tc_grid_widths_vs_oracle(F, width, os):
+@pytest.mark.parametrize("det", [False, True], ids=["atomic", "deterministic"])
+@pytest.mark.parametrize("width,os", [(2, 2.0), (3, 1.25), (4, 1.25), (5, 1.25), (6, 2.0)])
+def test_tc_grid_widths_vs_oracle(F, width, os, det):
+    """Widths 2..5 on the tensor cores (width 6 has no gridding bins and runs
+    on the CUDA cores); deterministic width 5 (bins of 3 x 2 x 2 cells, regions
+    of 7 x 6 x 6 points) has up to 3 covering bins per axis, the gather's
+    general path."""
     from oracle import nufft_ref as R
     from deepmr_b200 import synth
 
@@ -71,7 +76,10 @@ def test_tc_grid_widths_vs_oracle(F, width, os):
     plan = F.plan_nufft(c, n, width, os, device="cuda")
     ksp = synth.complex_gaussian((6,) + coord.shape[:-1], seed=width)
     ref = R.apply_nufft_adj(ksp, R.plan_nufft(c, n, width, os))
-    assert rel(_grid(F, plan, ksp.cuda()), ref) < TOL
+    x = _grid(F, plan, ksp.cuda(), det=det)
+    assert rel(x, ref) < TOL
+    if det:
+        assert torch.equal(x, _grid(F, plan, ksp.cuda(), det=True))
 
 
 def test_tc_grid_vs_deterministic(F):
